@@ -1,0 +1,274 @@
+#!/usr/bin/env python3
+"""Benchmark: PE grid-point updates/s of the split-step Pade range march on B200.
+
+Workload (default): the deep-water Munk batch - 4096 rays, per-ray frequency
+U[50,200] Hz and source depth U[50,1000] m, Munk sound speed with seeded
+Gaussian perturbations (sigma 2 m/s, 1 km correlation) every 5 km, flat 5000 m
+bottom, rmax 50 km, dr 25 m, dz 1 m, np 6, TL line output.  A "step" is one
+complete march of that batch (self-starter + all range steps of all rays).
+
+One grid-point update = one interior depth point of one ray advanced one range
+step with all np Pade terms; the count is sum_rays nz * nr (self-starter
+excluded).
+
+value : device time of the march (CUDA events on the engine's stream), inputs
+        already resident in HBM.
+e2e   : the same march through the C ABI call cr_run with host buffers: H2D of
+        the batch's inputs, the march, D2H of the TL / CP lines into pinned host
+        memory, every step; host wall clock around the call.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--form plain|chosen]
+       python bench.py --impl reference ...   (CPU restatement on host cores)
+Multi-GPU: launch with torch.distributed.run; every rank marches its own
+seeded batch of the same size (weak scaling, no collective on the data path).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "PE grid-point updates/s (1 B200) plain vs chosen form at ≤0.1 dB TL RMS error"
+UNIT = "grid-point updates/s"
+B_ALG = {"plain": 72.0, "chosen": 52.0}  # algorithmic bytes per grid-point update
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--form", choices=["plain", "chosen"], default="plain")
+    ap.add_argument("--rays", type=int, default=4096)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-rays", type=int, default=0, help="rays in the CPU sample (0: one per core)")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_config(a, batch):
+    return {"workload": f"Munk deep-water batch, {a.rays} rays per GPU, per-ray f U[50,200] Hz, "
+                        "zs U[50,1000] m, SSP updates every 5 km (sigma 2 m/s, 1 km corr.), "
+                        "5000 m flat, rmax 50 km, dr 25 m, dz 1 m, np 6, zr 500 m, TL line",
+            "rays_per_gpu": int(batch.n_rays), "form": a.form, "seed": a.seed,
+            "point_updates_per_gpu": batch.point_updates,
+            "nz_range": [int(batch.rays["nz"].min()), int(batch.rays["nz"].max())],
+            "steps_per_ray": int(batch.rays["nr"][0]),
+            "l2": "working set > L2 (column arrays ~1.6 GB per 4096 rays; no flush needed)"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.p is not None:
+            self.p.terminate()
+            try:
+                self.p.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        for line in Path(self.f.name).read_text().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": rows[0][1],
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return 6650.0, "fallback"
+
+
+def profiled_traffic(form):
+    """DRAM bytes per grid-point update of the march kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "march_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return float(d[form]["dram_bytes_per_point_update"])
+    except (KeyError, ValueError, TypeError):
+        return None
+
+
+def cpu_sample(batch, n_rays, seed, mode):
+    """Time the CPU restatement on a sample of the batch (one ray per core)."""
+    from oracle import oracle  # the CPU restatement; test/benchmark infrastructure only
+    rng = np.random.default_rng(seed)
+    cores = os.cpu_count() or 1
+    n = n_rays or cores
+    n = max(1, min(n, batch.n_rays))
+    pick = np.sort(rng.choice(batch.n_rays, size=n, replace=False))
+    work = float(np.sum(batch.rays["nz"][pick].astype(np.float64) * batch.rays["nr"][pick]))
+    t0 = time.perf_counter()
+    oracle.run(batch, mode, threads=min(cores, n), rays=pick)
+    dt = time.perf_counter() - t0
+    return work / dt, dt, n, min(cores, n)
+
+
+def run_reference(a):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    from cupyram_b200 import workloads
+    batch = workloads.build(*workloads.munk_batch(a.rays, seed=a.seed), compute_grids=False)
+    vals = []
+    for k in range(a.warmup + a.steps):
+        v, dt, n, cores = cpu_sample(batch, a.cpu_rays, a.seed + k, "ref")
+        if k >= a.warmup:
+            vals.append((v, dt))
+    value = float(np.mean([v for v, _ in vals]))
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": float(np.mean([dt for _, dt in vals]) * 1e3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+            "data": "synthetic", "impl": "reference", "config": workload_config(a, batch),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{n} rays of the batch per step, one ray per core, full march "
+                                       "each (the reference has no CPU path of its own: its kernels "
+                                       "are Numba CUDA; this is the C restatement in oracle/ "
+                                       "with the reference's float32/complex64 storage)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    a = parse()
+    if a.impl == "reference":
+        return run_reference(a)
+    rank, world, local = dist_env()
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    from cupyram_b200 import workloads
+    from cupyram_b200.engine import Engine
+    batch = workloads.build(*workloads.munk_batch(a.rays, seed=a.seed + 1000 * rank), compute_grids=False)
+    eng = Engine(batch, precision=a.form)
+    # pinned host output buffers for the end-to-end path
+    out = {"tll": torch.empty(batch.line_len, dtype=torch.float64, pin_memory=True),
+           "cpl": torch.empty(batch.line_len, dtype=torch.complex128, pin_memory=True)}
+
+    def barrier():
+        torch.cuda.synchronize()
+        if pg is not None:
+            pg.barrier()
+
+    for _ in range(a.warmup):
+        eng.run(out)
+    barrier()
+    march_ms, e2e_ms, h2d_b, d2h_b, launches = [], [], 0, 0, 0
+    with ClockSampler(local) as clk:
+        for _ in range(a.steps):
+            t0 = time.perf_counter()
+            eng.run(out)
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+            st = eng.stats()
+            march_ms.append(st["march_ms"])
+            h2d_b, d2h_b = st["h2d_bytes"], st["d2h_bytes"]
+            launches += st["kernel_launches"]
+    barrier()
+    t_march = float(np.sum(march_ms))
+    t_e2e = float(np.sum(e2e_ms))
+    if pg is not None:
+        t = torch.tensor([t_march, t_e2e], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        t_march, t_e2e = float(t[0]), float(t[1])
+    pu = batch.point_updates
+    total = pu * world * a.steps
+    value = total / (t_march * 1e-3)
+    e2e = total / (t_e2e * 1e-3)
+    # sanity: every ray's line is finite
+    tl = out["tll"].numpy()
+    if not np.all(np.isfinite(tl)):
+        raise RuntimeError("non-finite TL in the benchmark output")
+    if rank != 0:
+        if pg is not None:
+            pg.destroy_process_group()
+        return 0
+    peak, peak_kind = measured_peak_hbm()
+    per_launch_s = float(np.mean(march_ms)) * 1e-3
+    achieved = pu * B_ALG[a.form] / per_launch_s / 1e9
+    tpp = profiled_traffic(a.form)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": t_march / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "complex128" if a.form == "plain" else "complex64+fp64-refinement",
+            "data": "synthetic", "config": workload_config(a, batch),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "bytes_per_point_update": B_ALG[a.form],
+                         "traffic": (tpp * pu) if tpp else None},
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d_b),
+                    "d2h_bytes_per_step": int(d2h_b)},
+            "gpu_launches": int(launches), "clocks": clk.summary()}
+    if world == 1 and not a.no_cpu_baseline:
+        v, dt, n, cores = cpu_sample(batch, a.cpu_rays, a.seed, "plain")
+        line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": f"{n} of the {batch.n_rays} rays, full march each, one ray "
+                                          f"per core, {dt:.1f} s (C restatement in oracle/, FP64)"}
+    print(json.dumps(line), flush=True)
+    eng.close()
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,373 @@
+"""Host input pipeline: reference-style inputs -> packed per-ray batch description.
+
+This is the host half of ``CuPyRAM.__init__`` / ``CuPyRAM.setup`` of the
+reference (clapeyre/cupyram ``cupyram/cupyram.py``):
+
+* ``normalize_to_batch``  - ragged lists -> NaN-padded batches (``:56-120``)
+* ``valid_slice``         - strip NaN padding (``:123-174``)
+* ``check_inputs``        - per-ray validation, ``ValueError`` on bad input (``:382-458``)
+* ``derive_params``       - c0, lambda, dr, dz, zmplt, rmax, ns, rs, lyrw (``:460-526``)
+* ``build_batch``         - bathymetry extension, seabed offset, grid sizes,
+                            output sizes and the packed cr_ray / cr_env / pool
+                            arrays of the C ABI (``:528-726``)
+
+Two semantics are supported:
+
+* ``shared`` (the reference's): every calculation is an (environment,
+  frequency) pair of the cross product, and all share one grid whose nz,
+  dz, dr and absorbing layer come from the maximum frequency and the
+  deepest seabed of the batch.
+* ``per_ray`` (an extension for uneven batches): calculation i pairs
+  environment i with frequency i; source / receiver depth, dr, dz, np and
+  rmax may differ per ray and every ray gets its own grid (lambda_i = c0_i /
+  f_i).
+
+Deliberate differences from the reference (its defects, not its maths):
+range-dependence flags are taken per ray instead of from ray 0
+(``cupyram.py:437-442``), and the layer width uses each calculation's own
+lambda only in ``per_ray`` mode (shared mode keeps the reference's
+max-frequency lambda).
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._lib import ENV_DTYPE, MAX_NP, RAY_DTYPE
+
+ATTNF = 10.0  # attenuation at the bottom of the absorbing layer (cupyram.py:774)
+
+
+# ---------------------------------------------------------------------------
+# normalisation and NaN padding
+# ---------------------------------------------------------------------------
+def normalize_to_batch(x, batch_size, name):
+    """List -> stacked (or NaN-padded) batch; single array -> tiled batch."""
+    if isinstance(x, list):
+        if len(x) != batch_size:
+            raise ValueError(f"{name}: list length {len(x)} != batch_size {batch_size}")
+        arrays = [np.asarray(a) for a in x]
+        shapes = {a.shape for a in arrays}
+        if len(shapes) == 1:
+            return np.stack(arrays, axis=0)
+        ndim = arrays[0].ndim
+        if any(a.ndim != ndim for a in arrays):
+            raise ValueError(f"{name}: list entries differ in dimensionality")
+        max_shape = tuple(max(a.shape[i] for a in arrays) for i in range(ndim))
+        dtype = arrays[0].dtype
+        if np.issubdtype(dtype, np.integer) or dtype == bool:
+            dtype = np.float64
+        out = np.full((batch_size,) + max_shape, np.nan, dtype=dtype)
+        for i, a in enumerate(arrays):
+            out[(i,) + tuple(slice(0, s) for s in a.shape)] = a
+        return out
+    a = np.asarray(x)
+    if a.ndim == 0:
+        return np.full(batch_size, a)
+    return np.tile(a, (batch_size,) + (1,) * a.ndim)
+
+
+def valid_slice(arr):
+    """The non-NaN leading part of a padded 1-D or 2-D array (and its length)."""
+    arr = np.asarray(arr)
+    if arr.ndim == 1:
+        nan = np.isnan(arr)
+        if not nan.any():
+            return arr, len(arr)
+        n = int(np.argmax(nan))
+        return (arr[:n], n) if n > 0 else (arr, len(arr))
+    if arr.ndim == 2:
+        nan = np.isnan(arr)
+        rows = int(np.sum(~np.all(nan, axis=1)))
+        cols = int(np.sum(~np.all(nan, axis=0)))
+        if rows == arr.shape[0] and cols == arr.shape[1]:
+            return arr, arr.shape[0]
+        return arr[:rows, :cols], rows
+    flat = arr.reshape(arr.shape[0], -1)
+    bad = np.any(np.isnan(flat), axis=1)
+    if not bad.any():
+        return arr, len(arr)
+    n = int(np.argmax(bad))
+    return (arr[:n], n) if n > 0 else (arr, len(arr))
+
+
+# ---------------------------------------------------------------------------
+# per-ray environment record (valid parts only)
+# ---------------------------------------------------------------------------
+@dataclass
+class EnvRecord:
+    z_ss: np.ndarray
+    rp_ss: np.ndarray
+    cw: np.ndarray      # [n_zss, n_rss] (reference layout)
+    z_sb: np.ndarray    # relative to the deepest water-profile point (input form)
+    rp_sb: np.ndarray
+    cb: np.ndarray
+    rhob: np.ndarray
+    attn: np.ndarray
+    rbzb: np.ndarray    # [n_bt, 2]
+
+
+def check_inputs(n_env, zs, zr, z_ss, rp_ss, cw, z_sb, rp_sb, cb, rhob, attn, rbzb):
+    """Validate every environment; returns the list of EnvRecord (cupyram.py:382-434).
+
+    zs / zr are arrays of length n_env (the same value repeated in shared mode).
+    """
+    envs = []
+    for b in range(n_env):
+        zss = valid_slice(z_ss[b])[0].astype(np.float64)
+        rps = valid_slice(rp_ss[b])[0].astype(np.float64)
+        cwb = valid_slice(np.atleast_2d(cw[b]))[0].astype(np.float64)
+        zsb = valid_slice(z_sb[b])[0].astype(np.float64)
+        rpb = valid_slice(rp_sb[b])[0].astype(np.float64)
+        cbb = valid_slice(np.atleast_2d(cb[b]))[0].astype(np.float64)
+        rhb = valid_slice(np.atleast_2d(rhob[b]))[0].astype(np.float64)
+        atb = valid_slice(np.atleast_2d(attn[b]))[0].astype(np.float64)
+        bt = valid_slice(np.atleast_2d(rbzb[b]))[0].astype(np.float64)
+        if not (zss[0] <= zs[b] <= zss[-1]):
+            raise ValueError(f"Ray {b}: Source depth {zs[b]}m outside range [{zss[0]}, {zss[-1]}]m")
+        if not (zss[0] <= zr[b] <= zss[-1]):
+            raise ValueError(f"Ray {b}: Receiver depth {zr[b]}m outside range [{zss[0]}, {zss[-1]}]m")
+        if cwb.shape != (zss.size, rps.size):
+            raise ValueError(f"Ray {b}: z_ss ({zss.size}), rp_ss ({rps.size}), cw {cwb.shape} inconsistent")
+        for prof, name in ((cbb, "cb"), (rhb, "rhob"), (atb, "attn")):
+            if prof.shape != (zsb.size, rpb.size):
+                raise ValueError(f"Ray {b}: z_sb ({zsb.size}), rp_sb ({rpb.size}), {name} {prof.shape} inconsistent")
+        if bt.ndim != 2 or bt.shape[1] != 2:
+            raise ValueError(f"Ray {b}: rbzb must have two columns (range, depth)")
+        if bt[:, 1].max() > zss[-1]:
+            raise ValueError(f"Ray {b}: Max bathy ({bt[:, 1].max()}m) > max SSP depth ({zss[-1]}m)")
+        for arr, name in ((zss, "z_ss"), (rps, "rp_ss"), (zsb, "z_sb"), (rpb, "rp_sb"), (cwb, "cw"),
+                          (cbb, "cb"), (rhb, "rhob"), (atb, "attn"), (bt, "rbzb")):
+            if not np.all(np.isfinite(arr)):
+                raise ValueError(f"Ray {b}: {name} contains non-finite values inside its valid part")
+        if np.any(cwb <= 0) or np.any(cbb <= 0) or np.any(rhb <= 0):
+            raise ValueError(f"Ray {b}: sound speeds and densities must be positive")
+        envs.append(EnvRecord(zss, rps, cwb, zsb, rpb, cbb, rhb, atb, bt))
+    return envs
+
+
+# ---------------------------------------------------------------------------
+# parameters, grid and packing
+# ---------------------------------------------------------------------------
+@dataclass
+class Params:
+    np_pade: np.ndarray     # [n_calc] int
+    c0_env: np.ndarray      # [n_env]
+    c0_report: object       # 'c0' of the results dict
+    freqs: np.ndarray       # [n_freq] shared, or [n_calc] per-ray
+    dr: np.ndarray          # [n_calc]
+    dz: np.ndarray          # [n_calc]
+    ndr: int
+    ndz: int
+    zmplt: np.ndarray       # [n_calc]
+    rmax: np.ndarray        # [n_calc] (before truncation to whole output steps)
+    ns: int
+    rs: np.ndarray          # [n_calc]
+    lyrw: float
+    lam: np.ndarray         # [n_calc] wavelength used for the layer width
+    ident: object = 0
+
+
+def _per_calc(v, n, name, dtype=np.float64):
+    a = np.asarray(v, dtype=dtype)
+    if a.ndim == 0:
+        return np.full(n, a, dtype=dtype)
+    a = a.reshape(-1)
+    if a.size != n:
+        raise ValueError(f"{name}: expected a scalar or {n} values, got {a.size}")
+    return a
+
+
+@dataclass
+class Batch:
+    """Packed description ready for cr_create (plus what run() needs to reshape)."""
+    rays: np.ndarray
+    envs: np.ndarray
+    pool: np.ndarray
+    line_len: int
+    grid_len: int
+    compute_grids: bool
+    n_env: int
+    n_freq: int
+    per_ray: bool
+    nz: np.ndarray
+    nvr: np.ndarray
+    nvz: np.ndarray
+    zmax: np.ndarray
+    vr: list = field(default_factory=list)
+    vz: list = field(default_factory=list)
+
+    @property
+    def n_rays(self):
+        return len(self.rays)
+
+    @property
+    def point_updates(self):
+        return float(np.sum(self.rays["nz"].astype(np.float64) * self.rays["nr"]))
+
+
+def derive_params(envs, freqs, per_ray, kwargs, np_default=8, dzf=0.1, ndr_default=1,
+                  ndz_default=1, ns_default=1, lyrw_default=20, id_default=0):
+    """c0, lambda, dr, dz, zmplt, rmax, ns, rs (cupyram.py:460-526).
+
+    In shared mode every array is the same value repeated over the
+    n_env * n_freq calculations; in per-ray mode calculation i is env i.
+    """
+    n_env = len(envs)
+    n_freq = 1 if per_ray else len(freqs)
+    n_calc = n_env * n_freq
+    npp = _per_calc(kwargs.get("np", np_default), n_env if per_ray else 1, "np", np.int64)
+    if np.any(npp < 1) or np.any(npp > MAX_NP):
+        raise ValueError(f"np must be in 1..{MAX_NP}")
+    if "c0" in kwargs:
+        c0_env = _per_calc(kwargs["c0"], n_env, "c0")
+        c0_report = kwargs["c0"]
+    else:
+        c0_env = np.array([np.nanmean(e.cw[:, 0]) for e in envs])
+        c0_report = float(np.mean(c0_env))
+    if per_ray:
+        f = np.asarray(freqs, dtype=np.float64)
+        lam = c0_env / f
+        np_calc = npp if npp.size == n_env else np.full(n_env, int(npp[0]))
+        dr = _per_calc(kwargs["dr"], n_env, "dr") if "dr" in kwargs else np_calc * 1500.0 / f
+        dz = _per_calc(kwargs["dz"], n_env, "dz") if "dz" in kwargs else dzf * 1500.0 / f
+        zmplt = (_per_calc(kwargs["zmplt"], n_env, "zmplt") if "zmplt" in kwargs
+                 else np.array([e.rbzb[:, 1].max() for e in envs]))
+        rmax = (_per_calc(kwargs["rmax"], n_env, "rmax") if "rmax" in kwargs
+                else np.array([max(e.rp_ss.max(), e.rp_sb.max(), e.rbzb[:, 0].max()) for e in envs]))
+    else:
+        fmax = float(np.max(freqs))
+        c0_shared = float(np.mean(c0_env)) if "c0" not in kwargs else float(np.mean(c0_env))
+        np_calc = np.full(n_calc, int(npp[0]))
+        lam = np.full(n_calc, c0_shared / fmax)
+        dr = np.full(n_calc, float(kwargs.get("dr", int(npp[0]) * 1500.0 / fmax)))
+        dz = np.full(n_calc, float(kwargs.get("dz", dzf * 1500.0 / fmax)))
+        zmplt = np.full(n_calc, float(kwargs.get("zmplt", max(e.rbzb[:, 1].max() for e in envs))))
+        rmax_default = max(max(e.rp_ss.max(), e.rp_sb.max(), e.rbzb[:, 0].max()) for e in envs)
+        rmax = np.full(n_calc, float(kwargs.get("rmax", rmax_default)))
+    if np.any(dr <= 0) or np.any(dz <= 0):
+        raise ValueError("dr and dz must be positive")
+    ndr = int(kwargs.get("ndr", ndr_default))
+    ndz = int(kwargs.get("ndz", ndz_default))
+    if ndr < 1 or ndz < 1:
+        raise ValueError("ndr and ndz must be >= 1")
+    ns = int(kwargs.get("ns", ns_default))
+    if ns not in (0, 1, 2):
+        raise ValueError("ns must be 0, 1 or 2")
+    rs = _per_calc(kwargs["rs"], n_calc, "rs") if "rs" in kwargs else rmax + dr
+    lyrw = float(kwargs.get("lyrw", lyrw_default))
+    return Params(np_calc, c0_env, c0_report, np.asarray(freqs, dtype=np.float64), dr, dz, ndr, ndz,
+                  zmplt, rmax, ns, rs, lyrw, lam, kwargs.get("id", id_default))
+
+
+def build_batch(envs, p: Params, zs, zr, per_ray, compute_grids):
+    """Grid sizes, output sizes and the packed C-ABI arrays (cupyram.py:528-726).
+
+    zs, zr: per-environment arrays.
+    """
+    n_env = len(envs)
+    n_freq = 1 if per_ray else len(p.freqs)
+    n_calc = n_env * n_freq
+    # seabed depths are given relative to the deepest water-profile point
+    zsb_abs = [e.z_sb + e.z_ss[-1] for e in envs]
+    # bathymetry extended to rmax (the value before output truncation)
+    bt_ext = []
+    for k, e in enumerate(envs):
+        r_ext = p.rmax[k * n_freq]
+        bt = e.rbzb
+        if bt[-1, 0] < r_ext:
+            bt = np.vstack([bt, [r_ext, bt[-1, 1]]])
+        bt_ext.append(bt)
+    if per_ray:
+        zmax = np.array([zsb_abs[k].max() for k in range(n_env)]) + p.lyrw * p.lam
+    else:
+        zmax = np.full(n_calc, max(z.max() for z in zsb_abs) + p.lyrw * p.lam[0])
+    nz = (np.floor(zmax / p.dz) - 1).astype(np.int64)
+    nzplt = np.floor(p.zmplt / p.dz).astype(np.int64)
+    nvr = np.floor(p.rmax / (p.dr * p.ndr)).astype(np.int64)
+    rmax_t = nvr * p.dr * p.ndr
+    nvz = (nzplt // p.ndz).astype(np.int64)
+    nr = (np.round(rmax_t / p.dr) - 1).astype(np.int64)
+    if np.any(nz < 3):
+        raise ValueError("depth grid has fewer than 3 interior points; reduce dz")
+    if np.any(nvr < 1) or np.any(nr < 0):
+        raise ValueError("rmax must cover at least one output range step")
+
+    # pool: per env  z_ss, rp_ss, cw[n_rss][n_zss], z_sb, rp_sb, cb, rhob, attn, rb, zb
+    env_arr = np.zeros(n_env, dtype=ENV_DTYPE)
+    chunks = []
+    off = 0
+    for k, e in enumerate(envs):
+        parts = [e.z_ss, e.rp_ss, e.cw.T.reshape(-1), zsb_abs[k], e.rp_sb, e.cb.T.reshape(-1),
+                 e.rhob.T.reshape(-1), e.attn.T.reshape(-1), bt_ext[k][:, 0], bt_ext[k][:, 1]]
+        env_arr[k] = (e.z_ss.size, e.rp_ss.size, zsb_abs[k].size, e.rp_sb.size, bt_ext[k].shape[0], 0, off)
+        for q in parts:
+            chunks.append(np.ascontiguousarray(q, dtype=np.float64))
+            off += q.size
+    pool = np.concatenate(chunks) if chunks else np.zeros(1)
+
+    rays = np.zeros(n_calc, dtype=RAY_DTYPE)
+    line_off = 0
+    grid_off = 0
+    for b in range(n_calc):
+        e = b // n_freq
+        f = p.freqs[b] if per_ray else p.freqs[b % n_freq]
+        r = rays[b]
+        r["freq"] = f
+        r["c0"] = p.c0_env[e]
+        r["zs"] = zs[e]
+        r["zr"] = zr[e]
+        r["dz"] = p.dz[b]
+        r["dr"] = p.dr[b]
+        r["zmax"] = zmax[b]
+        r["lyrw_lambda"] = p.lyrw * p.lam[b]
+        r["attnf"] = ATTNF
+        r["rs"] = p.rs[b]
+        r["nz"] = nz[b]
+        r["nr"] = nr[b]
+        r["np"] = p.np_pade[b]
+        r["ns"] = p.ns
+        r["ndr"] = p.ndr
+        r["ndz"] = p.ndz
+        r["nvr"] = nvr[b]
+        r["nvz"] = nvz[b]
+        r["env"] = e
+        r["line_off"] = line_off
+        line_off += int(nvr[b])
+        if compute_grids:
+            r["grid_off"] = grid_off
+            grid_off += int(nvz[b] * nvr[b])
+        else:
+            r["grid_off"] = -1
+    for b in range(n_calc):
+        if int(np.floor(zs[b // n_freq] / p.dz[b])) + 1 > nz[b]:
+            raise ValueError(f"Ray {b}: source depth below the computational grid")
+    vr = [np.arange(1, nvr[b] + 1) * p.dr[b] * p.ndr for b in range(n_calc)]
+    vz = [np.arange(1, nvz[b] + 1) * p.dz[b] * p.ndz for b in range(n_calc)]
+    return Batch(rays, env_arr, pool, line_off, grid_off, bool(compute_grids), n_env, n_freq,
+                 per_ray, nz, nvr, nvz, zmax, vr, vz)
+
+
+def prepare(freq, zs, zr, z_ss, rp_ss, cw, z_sb, rp_sb, cb, rhob, attn, rbzb, kwargs):
+    """Full host pipeline; returns (envs, Params, zs_env, zr_env, per_ray)."""
+    per_ray = bool(kwargs.get("per_ray", False))
+    batch_size = int(kwargs.get("batch_size", 1))
+    if batch_size < 1:
+        raise ValueError("batch_size must be >= 1")
+    if np.isscalar(freq):
+        freqs = np.array([freq], dtype=np.float64)
+    else:
+        freqs = np.array(freq, dtype=np.float64).reshape(-1)
+    if freqs.size == 0 or np.any(~np.isfinite(freqs)) or np.any(freqs <= 0):
+        raise ValueError("freq must be positive")
+    if per_ray:
+        freqs = _per_calc(freqs if freqs.size > 1 else freqs[0], batch_size, "freq")
+    zs_env = _per_calc(zs, batch_size, "zs")
+    zr_env = _per_calc(zr, batch_size, "zr")
+    if not per_ray and (np.ndim(zs) or np.ndim(zr)):
+        raise ValueError("zs and zr must be scalars unless per_ray=True")
+    norm = [normalize_to_batch(x, batch_size, n) for x, n in
+            ((z_ss, "z_ss"), (rp_ss, "rp_ss"), (cw, "cw"), (z_sb, "z_sb"), (rp_sb, "rp_sb"),
+             (cb, "cb"), (rhob, "rhob"), (attn, "attn"), (rbzb, "rbzb"))]
+    envs = check_inputs(batch_size, zs_env, zr_env, *norm)
+    p = derive_params(envs, freqs, per_ray, kwargs)
+    return envs, p, zs_env, zr_env, per_ray

@@ -1,0 +1,54 @@
+"""Build the native engine in-tree: ``python -m cupyram_b200.build``.
+
+Compiles every ``csrc/*.cu`` for sm_100a (B200) into ``libcupyram_b200.so``
+next to this file.  nvcc cross-compiles, so no GPU is needed to build.
+"""
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+CSRC = HERE / "csrc"
+OUT = HERE / "libcupyram_b200.so"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
+         "--expt-relaxed-constexpr"]
+
+
+def nvcc():
+    cand = os.environ.get("NVCC") or shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not Path(cand).exists():
+        raise RuntimeError("nvcc not found; set NVCC or put CUDA's bin on PATH")
+    return cand
+
+
+def sources():
+    return sorted(CSRC.glob("*.cu"))
+
+
+def up_to_date():
+    if not OUT.exists():
+        return False
+    t = OUT.stat().st_mtime
+    deps = list(CSRC.glob("*")) + [HERE.parent / "include" / "cupyram_b200.h"]
+    return all(d.stat().st_mtime <= t for d in deps if d.exists())
+
+
+def build(force=False, verbose=False):
+    if not force and up_to_date():
+        return OUT
+    cmd = [nvcc(), *ARCH, *FLAGS, "-I", str(HERE.parent / "include"), "-o", str(OUT) + ".tmp",
+           *map(str, sources())]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(str(OUT) + ".tmp", OUT)
+    return OUT
+
+
+if __name__ == "__main__":
+    p = build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    print(p)

@@ -1,0 +1,1153 @@
+// engine.cu - B200 split-step Pade range march behind the cupyram_b200.h C ABI.
+//
+// Work decomposition
+//   * A "ray" is one calculation of the reference (an environment at one
+//     frequency).  Rays are sorted by work (rows x steps) and packed 32 to a
+//     tile; one warp marches one tile, one lane per ray.
+//   * Every per-row array of a tile is stored [row][lane] (32 consecutive
+//     lanes = 32 consecutive elements), so each load/store of a sweep is a
+//     fully coalesced warp access: 128 B (float), 256 B (float2) or 512 B
+//     (double2) per instruction.
+//   * The whole range march of a tile (self-starter, range-index updates,
+//     profile re-assembly, np Pade sweeps per step, receiver / TL-grid
+//     extraction) runs inside ONE kernel launch: the range loop is device
+//     resident, there is no per-step launch and no per-step host sync
+//     (the reference launches ~10 kernels and syncs 3 times per step).
+//
+// Sweep structure of one range step with n Pade terms (product form,
+// term j solves (M + pd2_j D) x = (M + pd1_j D) u):
+//   term j eliminates DOWN when j is even and UP when j is odd, so the back-
+//   substitution of term j runs in the same direction as the elimination of
+//   term j+1 and the two are fused into one pass over the column.  A step is
+//   n+1 passes instead of the reference's 2n, the field between terms never
+//   touches memory, and the Thomas workspace (w, g) of a row is overwritten
+//   in place one row behind the pass.
+//
+// References for the maths (clapeyre/cupyram):
+//   profile interpolation   cupyram/profl.py:8-140, cupyram/cupyram.py:770-803
+//   range-index update      cupyram/updat.py:38-140
+//   layer selection         cupyram/matrc.py:16-107 (iz == jz branch)
+//   Galerkin coefficients   cupyram/fused_kernel.py:20-69
+//   Thomas sweeps           cupyram/fused_kernel.py:72-153
+//   receiver / TL grid      cupyram/outpt.py:11-57
+//   self-starter            cupyram/cupyram.py:1001-1063
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <thread>
+#include <tuple>
+#include <vector>
+
+#include "../../include/cupyram_b200.h"
+#include "pade.h"
+
+namespace {
+
+constexpr int kTile = 32;  // rays per tile = lanes per warp
+
+// ---------------------------------------------------------------------------
+// device-side descriptors
+// ---------------------------------------------------------------------------
+struct RayDev {
+    double k0, omega, c0, dz, dr, zmax, lyrw_lambda, attnf, rs, zs, zr;
+    int nz, nr, np, ndr, ndz, nvr, nvz, env;
+    long long line_off, grid_off;
+    long long col;  // element index of (row 0, this lane) in the column arrays
+};
+
+struct EnvDev {
+    int n_zss, n_rss, n_zsb, n_rsb, n_bt, pad;
+    long long off;
+};
+
+// Pade sets per ray: 0 = (1-X)^-2 starter factor, 1 = starter ip=2,
+// 2 = march, 3 = march after the stability range rs.
+constexpr int kSets = 4;
+
+struct MarchArgs {
+    const RayDev* rays;
+    const int* tile_ray;  // [n_tiles * 32] -> ray index or -1
+    const EnvDev* envs;
+    const double* pool;
+    const double2* pd1;  // [ray][set][CR_MAX_NP]
+    const double2* pd2;
+    const int* pd_n;     // [ray][set]
+    float* f1;
+    float* f2;
+    float* f3;
+    float2* ksq;
+    double2* u;
+    double2* W;
+    double2* G;
+    double* tll;
+    double2* cpl;
+    double* tlg;
+    double2* cpg;
+    int* flags;
+    int compute_grids;
+};
+
+// ---------------------------------------------------------------------------
+// small complex helpers on double2
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double2 c2(double re, double im) { return make_double2(re, im); }
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return c2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 cfms(double2 acc, double2 a, double2 b) {  // acc - a*b
+    return c2(acc.x - fma(a.x, b.x, -a.y * b.y), acc.y - fma(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ double2 crcp(double2 b) {
+    const double inv = 1.0 / fma(b.x, b.x, b.y * b.y);
+    return c2(b.x * inv, -b.y * inv);
+}
+// a + p * d  with real a
+__device__ __forceinline__ double2 caxpd(double a, double2 p, double2 d) {
+    return c2(a + fma(p.x, d.x, -p.y * d.y), fma(p.x, d.y, p.y * d.x));
+}
+
+// ---------------------------------------------------------------------------
+// profile interpolation (profl)
+// ---------------------------------------------------------------------------
+struct EnvPtrs {
+    const double *z_ss, *rp_ss, *cw, *z_sb, *rp_sb, *cb, *rhob, *attn, *rb, *zb;
+    int n_zss, n_rss, n_zsb, n_rsb, n_bt;
+};
+
+__device__ EnvPtrs env_ptrs(const EnvDev& e, const double* pool) {
+    EnvPtrs p;
+    const double* q = pool + e.off;
+    p.n_zss = e.n_zss;
+    p.n_rss = e.n_rss;
+    p.n_zsb = e.n_zsb;
+    p.n_rsb = e.n_rsb;
+    p.n_bt = e.n_bt;
+    p.z_ss = q; q += p.n_zss;
+    p.rp_ss = q; q += p.n_rss;
+    p.cw = q; q += (long long)p.n_rss * p.n_zss;
+    p.z_sb = q; q += p.n_zsb;
+    p.rp_sb = q; q += p.n_rsb;
+    p.cb = q; q += (long long)p.n_rsb * p.n_zsb;
+    p.rhob = q; q += (long long)p.n_rsb * p.n_zsb;
+    p.attn = q; q += (long long)p.n_rsb * p.n_zsb;
+    p.rb = q; q += p.n_bt;
+    p.zb = q;
+    return p;
+}
+
+// index idx with arr[idx] <= v < arr[idx+1] (profl.py:8-35 semantics)
+__device__ __forceinline__ int seg_search(double v, const double* arr, int n) {
+    if (n <= 1 || v <= arr[0]) return 0;
+    if (v >= arr[n - 1]) return n - 2;
+    int lo = 0, hi = n - 1;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (arr[mid] <= v) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ double lerp_seg(double x, double x0, double x1, double y0, double y1) {
+    if (x1 == x0) return y0;
+    return y0 + (y1 - y0) * ((x - x0) / (x1 - x0));
+}
+
+struct RowProps {
+    float cw, cb, rhob, attn;
+};
+
+// Interpolated water / seabed properties at depth z for the active profiles,
+// rounded to float32 as the reference stores them.
+__device__ RowProps row_props(const EnvPtrs& e, int ss, int sb, double z, double lyrw_lambda,
+                              double attnf) {
+    RowProps o;
+    const double* cwp = e.cw + (long long)ss * e.n_zss;
+    const int n1 = e.n_zss;
+    double v;
+    if (z <= e.z_ss[0]) v = cwp[0];
+    else if (z >= e.z_ss[n1 - 1]) v = cwp[n1 - 1];
+    else {
+        const int k = seg_search(z, e.z_ss, n1);
+        v = lerp_seg(z, e.z_ss[k], e.z_ss[k + 1], cwp[k], cwp[k + 1]);
+    }
+    o.cw = (float)v;
+    const int n2 = e.n_zsb;
+    const long long so = (long long)sb * n2;
+    const double* cbp = e.cb + so;
+    const double* rhp = e.rhob + so;
+    const double* atp = e.attn + so;
+    const double z0 = e.z_sb[0], zl = e.z_sb[n2 - 1];
+    const int k = seg_search(z, e.z_sb, n2);
+    if (z <= z0) {
+        o.cb = (float)cbp[0];
+        o.rhob = (float)rhp[0];
+    } else if (z >= zl) {
+        o.cb = (float)cbp[n2 - 1];
+        o.rhob = (float)rhp[n2 - 1];
+    } else {
+        o.cb = (float)lerp_seg(z, e.z_sb[k], e.z_sb[k + 1], cbp[k], cbp[k + 1]);
+        o.rhob = (float)lerp_seg(z, e.z_sb[k], e.z_sb[k + 1], rhp[k], rhp[k + 1]);
+    }
+    // attenuation with the absorbing layer: profile, then constant over the
+    // first 75 % of the layer, then a linear ramp to attnf (profl.py:121-140)
+    const double alast = atp[n2 - 1];
+    const double zl1 = zl + 0.75 * lyrw_lambda, zl2 = zl + lyrw_lambda;
+    if (z <= zl) {
+        if (z <= z0) v = atp[0];
+        else v = lerp_seg(z, e.z_sb[k], e.z_sb[k + 1], atp[k], atp[k + 1]);
+    } else if (z <= zl1) {
+        v = alast;
+    } else if (z <= zl2) {
+        v = lerp_seg(z, zl1, zl2, alast, attnf);
+    } else {
+        v = attnf;
+    }
+    o.attn = (float)v;
+    return o;
+}
+
+// Write the layer-selected coefficients of rows [lo, hi] (matrc.py:16-107
+// with iz == jz, preceded by the alpw / alpb / ksqw / ksqb maths of
+// cupyram.py:782-803).
+__device__ void assemble_rows(const RayDev& ry, const EnvPtrs& e, int ss, int sb, int iz, int lo,
+                              int hi, float* f1, float* f2, float* f3, float2* ksq) {
+    const double step = ry.zmax / (double)(ry.nz + 1);
+    const double eta = 1.0 / (40.0 * M_PI * 0.43429448190325176);  // 1/(40 pi log10 e)
+    const double k02 = ry.k0 * ry.k0;
+    for (int i = lo; i <= hi; ++i) {
+        const double z = (i == ry.nz + 1) ? ry.zmax : (double)i * step;
+        const RowProps p = row_props(e, ss, sb, z, ry.lyrw_lambda, ry.attnf);
+        const long long o = ry.col + (long long)i * kTile;
+        if (i <= iz) {
+            const double alpw = sqrt((double)p.cw / ry.c0);
+            const double ow = ry.omega / (double)p.cw;
+            f1[o] = (float)(1.0 / alpw);
+            f2[o] = 1.0f;
+            f3[o] = (float)alpw;
+            ksq[o] = make_float2((float)(ow * ow - k02), 0.0f);
+        } else {
+            const double alpb = sqrt((double)(p.rhob * p.cb) / ry.c0);
+            const double ob = ry.omega / (double)p.cb;
+            const double ti = ob * eta * (double)p.attn;  // term = ob + i*ti
+            f1[o] = (float)((double)p.rhob / alpb);
+            f2[o] = (float)(1.0 / (double)p.rhob);
+            f3[o] = (float)alpb;
+            ksq[o] = make_float2((float)(ob * ob - ti * ti - k02), (float)(2.0 * ob * ti));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Galerkin row: D_i = (d1, d2, d3) from the 3-row window of f1..f3, ksq
+// ---------------------------------------------------------------------------
+struct Win {
+    float f1c, f2m, f2c, f2p, f3m, f3c, f3p;
+    float2 km, kc, kp;
+};
+
+struct Drow {
+    double2 d1, d2, d3;
+};
+
+__device__ __forceinline__ Drow galerkin(const Win& w, double cfact) {
+    const double f1 = w.f1c;
+    const double c1 = cfact * f1 * ((double)w.f2m + (double)w.f2c) * (double)w.f3m;
+    const double c2v = -cfact * f1 * ((double)w.f2m + 2.0 * (double)w.f2c + (double)w.f2p) * (double)w.f3c;
+    const double c3 = cfact * f1 * ((double)w.f2c + (double)w.f2p) * (double)w.f3p;
+    const double df = 1.0 / 12.0;
+    Drow d;
+    d.d1 = c2(c1 + df * ((double)w.km.x + (double)w.kc.x), df * ((double)w.km.y + (double)w.kc.y));
+    d.d2 = c2(c2v + df * ((double)w.km.x + 6.0 * (double)w.kc.x + (double)w.kp.x),
+              df * ((double)w.km.y + 6.0 * (double)w.kc.y + (double)w.kp.y));
+    d.d3 = c2(c3 + df * ((double)w.kc.x + (double)w.kp.x), df * ((double)w.kc.y + (double)w.kp.y));
+    return d;
+}
+
+struct Col {
+    const float* f1;
+    const float* f2;
+    const float* f3;
+    const float2* ksq;
+    double2* u;
+    double2* W;
+    double2* G;
+};
+
+struct StepCtx {
+    Col c;
+    int nz;
+    double cfact, a1, a2;
+    double2 u0;  // field value held at the surface row (non-zero only for zs < dz)
+};
+
+// ---------------------------------------------------------------------------
+// the passes of one range step
+// ---------------------------------------------------------------------------
+// Pass 0: eliminate term 0 downwards reading the step's input field.
+__device__ void pass_first(const StepCtx& s, double2 p1, double2 p2) {
+    const Col& c = s.c;
+    const int nz = s.nz;
+    Win w;
+    w.f2m = c.f2[0];
+    w.f3m = c.f3[0];
+    w.km = c.ksq[0];
+    w.f1c = c.f1[kTile];
+    w.f2c = c.f2[kTile];
+    w.f3c = c.f3[kTile];
+    w.kc = c.ksq[kTile];
+    double2 xm = s.u0, xc = c.u[kTile];
+    double2 wp = c2(0.0, 0.0), gp = c2(0.0, 0.0);
+    for (int i = 1; i <= nz; ++i) {
+        const long long o = (long long)(i + 1) * kTile;
+        w.f2p = c.f2[o];
+        w.f3p = c.f3[o];
+        w.kp = c.ksq[o];
+        const double2 xp = (i < nz) ? c.u[o] : c2(0.0, 0.0);
+        const float f1n = c.f1[o];
+        const Drow d = galerkin(w, s.cfact);
+        const double2 r1 = caxpd(s.a1, p2, d.d1), r2 = caxpd(s.a2, p2, d.d2), r3 = caxpd(s.a1, p2, d.d3);
+        const double2 q1 = caxpd(s.a1, p1, d.d1), q2 = caxpd(s.a2, p1, d.d2), q3 = caxpd(s.a1, p1, d.d3);
+        double2 rhs = cmul(q1, xm);
+        rhs = c2(rhs.x + (q2.x * xc.x - q2.y * xc.y) + (q3.x * xp.x - q3.y * xp.y),
+                 rhs.y + (q2.x * xc.y + q2.y * xc.x) + (q3.x * xp.y + q3.y * xp.x));
+        const double2 inv = crcp(cfms(r2, r1, wp));
+        wp = cmul(r3, inv);
+        gp = cmul(cfms(rhs, r1, gp), inv);
+        const long long oi = (long long)i * kTile;
+        c.W[oi] = wp;
+        c.G[oi] = gp;
+        xm = xc;
+        xc = xp;
+        w.f2m = w.f2c; w.f3m = w.f3c; w.km = w.kc;
+        w.f1c = f1n; w.f2c = w.f2p; w.f3c = w.f3p; w.kc = w.kp;
+    }
+}
+
+// Fused pass going DOWN: back-substitute a term that was eliminated UP
+// (x_i = g_i - w_i x_{i-1}) and eliminate the next term DOWN one row behind.
+__device__ void pass_fused_down(const StepCtx& s, double2 p1, double2 p2) {
+    const Col& c = s.c;
+    const int nz = s.nz;
+    Win w;
+    w.f2m = c.f2[0];
+    w.f3m = c.f3[0];
+    w.km = c.ksq[0];
+    w.f1c = c.f1[kTile];
+    w.f2c = c.f2[kTile];
+    w.f3c = c.f3[kTile];
+    w.kc = c.ksq[kTile];
+    double2 xmm = s.u0;  // x_{i-2}
+    double2 xm = s.u0;   // x_{i-1}; at i = 1 the back-substitution starts from x_0
+    double2 wp = c2(0.0, 0.0), gp = c2(0.0, 0.0);
+    // back-substitution of the previous term: x_1 = g'_1, x_i = g'_i - w'_i x_{i-1}
+    for (int i = 1; i <= nz + 1; ++i) {
+        double2 xc;
+        if (i <= nz) {
+            const long long oi = (long long)i * kTile;
+            const double2 wi = c.W[oi], gi = c.G[oi];
+            xc = (i == 1) ? gi : cfms(gi, wi, xm);
+        } else {
+            xc = c2(0.0, 0.0);
+        }
+        if (i >= 2) {
+            // eliminate row m = i-1 (needs x_{m-1} = xmm, x_m = xm, x_{m+1} = xc)
+            const int m = i - 1;
+            const long long o = (long long)(m + 1) * kTile;
+            w.f2p = c.f2[o];
+            w.f3p = c.f3[o];
+            w.kp = c.ksq[o];
+            const float f1n = (m + 1 <= nz + 1) ? c.f1[o] : 0.0f;
+            const Drow d = galerkin(w, s.cfact);
+            const double2 r1 = caxpd(s.a1, p2, d.d1), r2 = caxpd(s.a2, p2, d.d2), r3 = caxpd(s.a1, p2, d.d3);
+            const double2 q1 = caxpd(s.a1, p1, d.d1), q2 = caxpd(s.a2, p1, d.d2), q3 = caxpd(s.a1, p1, d.d3);
+            double2 rhs = cmul(q1, xmm);
+            rhs = c2(rhs.x + (q2.x * xm.x - q2.y * xm.y) + (q3.x * xc.x - q3.y * xc.y),
+                     rhs.y + (q2.x * xm.y + q2.y * xm.x) + (q3.x * xc.y + q3.y * xc.x));
+            const double2 inv = crcp(cfms(r2, r1, wp));
+            wp = cmul(r3, inv);
+            gp = cmul(cfms(rhs, r1, gp), inv);
+            const long long om = (long long)m * kTile;
+            c.W[om] = wp;
+            c.G[om] = gp;
+            w.f2m = w.f2c; w.f3m = w.f3c; w.km = w.kc;
+            w.f1c = f1n; w.f2c = w.f2p; w.f3c = w.f3p; w.kc = w.kp;
+        }
+        xmm = xm;
+        xm = xc;
+    }
+}
+
+// Fused pass going UP: back-substitute a term eliminated DOWN
+// (x_i = g_i - w_i x_{i+1}) and eliminate the next term UP one row behind.
+__device__ void pass_fused_up(const StepCtx& s, double2 p1, double2 p2) {
+    const Col& c = s.c;
+    const int nz = s.nz;
+    // Window rows (m-1, m, m+1) for m = i+1 once row i is loaded.  Each
+    // iteration rotates p <- c <- m <- (row i); the "m" slot starts with row
+    // nz+1 so that the first elimination (m = nz) sees rows nz-1, nz, nz+1.
+    Win w;
+    {
+        const long long o = (long long)(nz + 1) * kTile;
+        w.f2m = c.f2[o];
+        w.f3m = c.f3[o];
+        w.km = c.ksq[o];
+        w.f1c = 0.0f;
+        w.f2c = 0.0f; w.f3c = 0.0f; w.kc = make_float2(0.f, 0.f);
+        w.f2p = 0.0f; w.f3p = 0.0f; w.kp = make_float2(0.f, 0.f);
+    }
+    double2 xpp = c2(0.0, 0.0);  // x_{i+2}
+    double2 xp = c2(0.0, 0.0);   // x_{i+1}
+    double2 wp = c2(0.0, 0.0), gp = c2(0.0, 0.0);
+    for (int i = nz; i >= 0; --i) {
+        double2 xc;
+        if (i >= 1) {
+            const long long oi = (long long)i * kTile;
+            const double2 wi = c.W[oi], gi = c.G[oi];
+            xc = (i == nz) ? gi : cfms(gi, wi, xp);
+        } else {
+            xc = s.u0;
+        }
+        // slide the window down one row: load row i as the new "m-1"
+        const long long o = (long long)i * kTile;
+        const float f1i = c.f1[o];
+        const float f2i = c.f2[o];
+        const float f3i = c.f3[o];
+        const float2 ki = c.ksq[o];
+        w.f2p = w.f2c; w.f3p = w.f3c; w.kp = w.kc;
+        w.f2c = w.f2m; w.f3c = w.f3m; w.kc = w.km;  // (previous "m-1" becomes "m")
+        w.f2m = f2i; w.f3m = f3i; w.km = ki;
+        const float f1m_next = f1i;
+        if (i <= nz - 1) {
+            // eliminate row m = i+1 (needs x_i = xc, x_{m} = xp, x_{m+1} = xpp)
+            const int m = i + 1;
+            const Drow d = galerkin(w, s.cfact);
+            const double2 r1 = caxpd(s.a1, p2, d.d1), r2 = caxpd(s.a2, p2, d.d2), r3 = caxpd(s.a1, p2, d.d3);
+            const double2 q1 = caxpd(s.a1, p1, d.d1), q2 = caxpd(s.a2, p1, d.d2), q3 = caxpd(s.a1, p1, d.d3);
+            double2 rhs = cmul(q1, xc);
+            rhs = c2(rhs.x + (q2.x * xp.x - q2.y * xp.y) + (q3.x * xpp.x - q3.y * xpp.y),
+                     rhs.y + (q2.x * xp.y + q2.y * xp.x) + (q3.x * xpp.y + q3.y * xpp.x));
+            const double2 inv = crcp(cfms(r2, r3, wp));
+            wp = cmul(r1, inv);
+            gp = cmul(cfms(rhs, r3, gp), inv);
+            const long long om = (long long)m * kTile;
+            c.W[om] = wp;
+            c.G[om] = gp;
+        }
+        w.f1c = f1m_next;  // f1 of the row that becomes "m" at the next iteration
+        xpp = xp;
+        xp = xc;
+    }
+}
+
+// Last pass: back-substitute the last term and store the field.
+__device__ void pass_last(const StepCtx& s, bool last_elim_down) {
+    const Col& c = s.c;
+    const int nz = s.nz;
+    if (last_elim_down) {
+        double2 xp = c2(0.0, 0.0);
+        for (int i = nz; i >= 1; --i) {
+            const long long oi = (long long)i * kTile;
+            const double2 gi = c.G[oi];
+            const double2 xc = (i == nz) ? gi : cfms(gi, c.W[oi], xp);
+            c.u[oi] = xc;
+            xp = xc;
+        }
+    } else {
+        double2 xm = s.u0;
+        for (int i = 1; i <= nz; ++i) {
+            const long long oi = (long long)i * kTile;
+            const double2 gi = c.G[oi];
+            const double2 xc = (i == 1) ? gi : cfms(gi, c.W[oi], xm);
+            c.u[oi] = xc;
+            xm = xc;
+        }
+    }
+}
+
+// Pass 0 with the elimination running UP is never needed: term 0 always
+// eliminates DOWN.  The eliminations go DOWN for even terms, UP for odd ones.
+__device__ void pe_step(const StepCtx& s, const double2* p1, const double2* p2, int n) {
+    pass_first(s, p1[0], p2[0]);
+    for (int t = 1; t < n; ++t) {
+        if (t & 1) pass_fused_up(s, p1[t], p2[t]);
+        else pass_fused_down(s, p1[t], p2[t]);
+    }
+    pass_last(s, ((n - 1) & 1) == 0);
+}
+
+__device__ __forceinline__ double tl_db(double amp, double r) {
+    return -20.0 * log10(amp + 1e-20) + 10.0 * log10(r + 1e-20);
+}
+
+// Receiver line and TL grid after a step (outpt.py:11-57).  The CP grid is
+// filled as well (the reference allocates it but never writes it).
+__device__ void write_outputs(const MarchArgs& a, const RayDev& ry, const Col& c, double2 u0,
+                              int tlc, double r, int ir, double dir, int* flag) {
+    auto urow = [&](int i) -> double2 {
+        if (i <= 0) return u0;
+        if (i > ry.nz) return c2(0.0, 0.0);
+        return c.u[(long long)i * kTile];
+    };
+    const double2 ua = urow(ir), ub = urow(ir + 1);
+    const double fa = c.f3[(long long)ir * kTile];
+    const double fb = c.f3[(long long)(ir + 1) * kTile];
+    const double2 cp = c2((1.0 - dir) * fa * ua.x + dir * fb * ub.x, (1.0 - dir) * fa * ua.y + dir * fb * ub.y);
+    const double amp = hypot(cp.x, cp.y);
+    if (!isfinite(amp)) *flag |= 1;
+    a.tll[ry.line_off + tlc] = tl_db(amp, r);
+    a.cpl[ry.line_off + tlc] = cp;
+    if (a.compute_grids && ry.grid_off >= 0) {
+        for (int k = 0; k < ry.nvz; ++k) {
+            const int j = (k + 1) * ry.ndz;
+            if (j > ry.nz + 1) break;
+            const double2 uj = urow(j);
+            const double fj = c.f3[(long long)j * kTile];
+            const double2 g = c2(uj.x * fj, uj.y * fj);
+            const long long o = ry.grid_off + (long long)k * ry.nvr + tlc;
+            a.tlg[o] = tl_db(hypot(g.x, g.y), r);
+            a.cpg[o] = g;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// the march kernel: one lane = one ray, all steps
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kTile) march_kernel(MarchArgs a) {
+    const int rid = a.tile_ray[blockIdx.x * kTile + threadIdx.x];
+    if (rid < 0) return;
+    const RayDev ry = a.rays[rid];
+    const EnvPtrs e = env_ptrs(a.envs[ry.env], a.pool);
+    Col c;
+    c.f1 = a.f1 + ry.col;
+    c.f2 = a.f2 + ry.col;
+    c.f3 = a.f3 + ry.col;
+    c.ksq = a.ksq + ry.col;
+    c.u = a.u + ry.col;
+    c.W = a.W + ry.col;
+    c.G = a.G + ry.col;
+    const int nz = ry.nz;
+    int flag = 0;
+
+    // initial indices (cupyram.py:571-608)
+    int iz = (int)floor(e.zb[0] / ry.dz);
+    iz = max(1, min(nz - 1, iz));
+    int ss = 0, sb = 0, bt = 0;
+    assemble_rows(ry, e, ss, sb, iz, 0, nz + 1, a.f1, a.f2, a.f3, a.ksq);
+
+    StepCtx s;
+    s.c = c;
+    s.nz = nz;
+    s.cfact = 0.5 / (ry.dz * ry.dz);
+    s.a1 = ry.k0 * ry.k0 / 6.0;
+    s.a2 = 2.0 * ry.k0 * ry.k0 / 3.0;
+
+    // self-starter: delta at zs split over two rows, divided by (1-X)^2
+    // (two passes of the pd1 = 0, pd2 = -1 operator), then the ip = 2 operator
+    for (int i = 0; i <= nz + 1; ++i) c.u[(long long)i * kTile] = c2(0.0, 0.0);
+    {
+        const double si = ry.zs / ry.dz;
+        const int is = (int)floor(si);
+        const double dis = si - is;
+        const double amp = sqrt(2.0 * M_PI / ry.k0);
+        const double step = ry.zmax / (double)(nz + 1);
+        for (int k = 0; k < 2; ++k) {
+            const int i = is + k;
+            const double z = (i == nz + 1) ? ry.zmax : (double)i * step;
+            const RowProps p = row_props(e, ss, sb, z, ry.lyrw_lambda, ry.attnf);
+            const double alpw = sqrt((double)p.cw / ry.c0);
+            const double wgt = (k == 0) ? (1.0 - dis) : dis;
+            c.u[(long long)i * kTile] = c2(wgt * amp / (ry.dz * alpw), 0.0);
+        }
+        s.u0 = c.u[0];
+    }
+    const double2* pd1 = a.pd1 + (long long)rid * kSets * CR_MAX_NP;
+    const double2* pd2 = a.pd2 + (long long)rid * kSets * CR_MAX_NP;
+    const int* pn = a.pd_n + rid * kSets;
+    pe_step(s, pd1, pd2, pn[0]);
+    pe_step(s, pd1, pd2, pn[0]);
+    pe_step(s, pd1 + CR_MAX_NP, pd2 + CR_MAX_NP, pn[1]);
+
+    const double ri = ry.zr / ry.dz;
+    const int ir = (int)floor(ri);
+    const double dir = ri - ir;
+    int mdr = 0, tlc = -1;
+    double r = ry.dr;
+    if (++mdr == ry.ndr) {
+        mdr = 0;
+        ++tlc;
+        if (tlc < ry.nvr) write_outputs(a, ry, c, s.u0, tlc, r, ir, dir, &flag);
+    }
+
+    int set = 2;
+    double rs = ry.rs;
+    for (int rn = 0; rn < ry.nr; ++rn) {
+        // updat (updat.py:38-140): bathymetry index at r + dr/2, profile indices at r
+        bool reprofile = false;
+        int iz_new = iz;
+        if (e.n_bt > 1) {
+            while (bt < e.n_bt - 1 && r >= e.rb[bt + 1]) ++bt;
+            const int b1 = min(bt + 1, e.n_bt - 1);
+            const double r0 = e.rb[bt], r1 = e.rb[b1], z0 = e.zb[bt], z1 = e.zb[b1];
+            const double zc = (b1 == bt) ? z0 : z0 + (r + 0.5 * ry.dr - r0) * (z1 - z0) / (r1 - r0);
+            iz_new = max(1, min(nz - 1, (int)floor(zc / ry.dz)));
+        }
+        if (e.n_rss > 1) {
+            const int o = ss;
+            while (ss < e.n_rss - 1 && r >= e.rp_ss[ss + 1]) ++ss;
+            reprofile |= (ss != o);
+        }
+        if (e.n_rsb > 1) {
+            const int o = sb;
+            while (sb < e.n_rsb - 1 && r >= e.rp_sb[sb + 1]) ++sb;
+            reprofile |= (sb != o);
+        }
+        if (reprofile) {
+            assemble_rows(ry, e, ss, sb, iz_new, 0, nz + 1, a.f1, a.f2, a.f3, a.ksq);
+        } else if (iz_new != iz) {
+            // only the rows that change layer
+            assemble_rows(ry, e, ss, sb, iz_new, min(iz, iz_new) + 1, max(iz, iz_new), a.f1, a.f2,
+                          a.f3, a.ksq);
+        }
+        iz = iz_new;
+        if (r >= rs) {  // stability constraints off (cupyram.py:976-999)
+            set = 3;
+            rs = INFINITY;
+        }
+        pe_step(s, pd1 + set * CR_MAX_NP, pd2 + set * CR_MAX_NP, pn[set]);
+        r = (double)(rn + 2) * ry.dr;
+        if (++mdr == ry.ndr) {
+            mdr = 0;
+            ++tlc;
+            if (tlc < ry.nvr) write_outputs(a, ry, c, s.u0, tlc, r, ir, dir, &flag);
+        }
+    }
+    a.flags[rid] = flag;
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+thread_local std::string g_error;
+
+void set_global_error(const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_error = buf;
+}
+
+}  // namespace
+
+struct cr_engine {
+    std::string err;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    int n_rays = 0, n_envs = 0, n_tiles = 0;
+    int precision = 0, compute_grids = 0;
+    long long line_len = 0, grid_len = 0, pool_len = 0;
+    long long col_elems = 0;
+    double point_updates = 0.0;
+    // host copies
+    std::vector<RayDev> rays;
+    std::vector<EnvDev> envs;
+    std::vector<double> pool;
+    std::vector<int> tile_ray;
+    std::vector<double2> pd1, pd2;
+    std::vector<int> pd_n;
+    // device buffers
+    RayDev* d_rays = nullptr;
+    EnvDev* d_envs = nullptr;
+    double* d_pool = nullptr;
+    int* d_tile_ray = nullptr;
+    double2 *d_pd1 = nullptr, *d_pd2 = nullptr;
+    int* d_pd_n = nullptr;
+    float *d_f1 = nullptr, *d_f2 = nullptr, *d_f3 = nullptr;
+    float2* d_ksq = nullptr;
+    double2 *d_u = nullptr, *d_W = nullptr, *d_G = nullptr;
+    double* d_tll = nullptr;
+    double2* d_cpl = nullptr;
+    double* d_tlg = nullptr;
+    double2* d_cpg = nullptr;
+    int* d_flags = nullptr;
+    long long device_bytes = 0;
+    bool uploaded = false, marched = false;
+    cr_stats st{};
+
+    int fail(int code, const char* fmt, ...) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof buf, fmt, ap);
+        va_end(ap);
+        err = buf;
+        return code;
+    }
+    int cuda_fail(cudaError_t e, const char* what) {
+        return fail(e == cudaErrorMemoryAllocation ? CR_ENOMEM : CR_ECUDA, "%s: %s", what,
+                    cudaGetErrorString(e));
+    }
+};
+
+namespace {
+
+template <typename T>
+cudaError_t dev_alloc(cr_engine* e, T** p, size_t count) {
+    if (count == 0) count = 1;
+    const size_t bytes = count * sizeof(T);
+    cudaError_t rc = cudaMalloc((void**)p, bytes);
+    if (rc == cudaSuccess) e->device_bytes += (long long)bytes;
+    return rc;
+}
+
+void free_all(cr_engine* e) {
+    void* ptrs[] = {e->d_rays, e->d_envs, e->d_pool, e->d_tile_ray, e->d_pd1, e->d_pd2, e->d_pd_n,
+                    e->d_f1,   e->d_f2,   e->d_f3,   e->d_ksq,      e->d_u,   e->d_W,   e->d_G,
+                    e->d_tll,  e->d_cpl,  e->d_tlg,  e->d_cpg,      e->d_flags};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    for (auto& ev : e->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (e->stream) cudaStreamDestroy(e->stream);
+}
+
+// Validate the batch; returns an error message or empty string.
+std::string validate(const cr_batch* b) {
+    char buf[256];
+    if (!b) return "batch is NULL";
+    if (b->n_rays < 1) return "n_rays must be >= 1";
+    if (b->n_envs < 1) return "n_envs must be >= 1";
+    if (!b->rays || !b->envs || !b->pool) return "rays, envs and pool must be non-NULL";
+    if (b->precision != CR_PLAIN_C128 && b->precision != CR_CHOSEN_C64R) return "unknown precision form";
+    for (int k = 0; k < b->n_envs; ++k) {
+        const cr_env& v = b->envs[k];
+        if (v.n_zss < 1 || v.n_rss < 1 || v.n_zsb < 1 || v.n_rsb < 1 || v.n_bt < 1) {
+            snprintf(buf, sizeof buf, "environment %d has an empty profile or bathymetry", k);
+            return buf;
+        }
+        const long long need = (long long)v.n_zss + v.n_rss + (long long)v.n_rss * v.n_zss + v.n_zsb +
+                               v.n_rsb + 3LL * v.n_rsb * v.n_zsb + 2LL * v.n_bt;
+        if (v.off < 0 || v.off + need > b->pool_len) {
+            snprintf(buf, sizeof buf, "environment %d overruns the pool", k);
+            return buf;
+        }
+    }
+    for (int i = 0; i < b->n_rays; ++i) {
+        const cr_ray& r = b->rays[i];
+        auto bad = [&](const char* what) {
+            snprintf(buf, sizeof buf, "ray %d: %s", i, what);
+            return std::string(buf);
+        };
+        if (r.env < 0 || r.env >= b->n_envs) return bad("env index out of range");
+        if (!(r.freq > 0) || !(r.c0 > 0)) return bad("freq and c0 must be > 0");
+        if (!(r.dz > 0) || !(r.dr > 0)) return bad("dz and dr must be > 0");
+        if (r.nz < 3) return bad("nz must be >= 3");
+        if (r.nr < 0) return bad("nr must be >= 0");
+        if (r.np < 1 || r.np > CR_MAX_NP) return bad("np out of range");
+        if (r.ns < 0 || r.ns > 2) return bad("ns must be 0, 1 or 2");
+        if (r.ndr < 1 || r.ndz < 1) return bad("ndr and ndz must be >= 1");
+        if (r.nvr < 0 || r.nvz < 0) return bad("nvr and nvz must be >= 0");
+        if (!(r.zs >= 0) || (int)std::floor(r.zs / r.dz) + 1 > r.nz) return bad("source depth outside the grid");
+        if (!(r.zr >= 0) || (int)std::floor(r.zr / r.dz) + 1 > r.nz + 1) return bad("receiver depth outside the grid");
+        if (r.line_off < 0 || r.line_off + r.nvr > b->line_len) return bad("TL line overruns line_len");
+        if (b->compute_grids && r.grid_off >= 0 && r.grid_off + (long long)r.nvz * r.nvr > b->grid_len)
+            return bad("TL grid overruns grid_len");
+        if ((long long)(r.nvr) * r.ndr > (long long)r.nr + 1) return bad("nvr * ndr exceeds nr + 1 outputs");
+    }
+    return std::string();
+}
+
+// Pade sets for every ray; identical (freq, c0, np, ns, dr) share one solve.
+int compute_pade_sets(cr_engine* e, const cr_batch* b) {
+    using Key = std::tuple<double, double, int, int, double>;
+    std::map<Key, int> uniq;
+    std::vector<Key> keys;
+    std::vector<int> ray_key(b->n_rays);
+    for (int i = 0; i < b->n_rays; ++i) {
+        const cr_ray& r = b->rays[i];
+        Key k{r.freq, r.c0, r.np, r.ns, r.dr};
+        auto it = uniq.find(k);
+        if (it == uniq.end()) {
+            it = uniq.emplace(k, (int)keys.size()).first;
+            keys.push_back(k);
+        }
+        ray_key[i] = it->second;
+    }
+    const int nk = (int)keys.size();
+    // per key: set1 (ip=2), set2 (ip=1, ns), set3 (ip=1, ns=0)
+    std::vector<cr::cd> res((size_t)nk * 3 * 2 * CR_MAX_NP);
+    std::vector<int> status(nk, 0);
+    std::atomic<int> next{0};
+    auto work = [&]() {
+        for (;;) {
+            const int k = next.fetch_add(1);
+            if (k >= nk) return;
+            const auto& [freq, c0, np, ns, dr] = keys[k];
+            cr::cd* base = res.data() + (size_t)k * 3 * 2 * CR_MAX_NP;
+            int rc = cr::pade_coefficients(freq, c0, np, ns, dr, 2, base, base + CR_MAX_NP);
+            if (!rc) rc = cr::pade_coefficients(freq, c0, np, ns, dr, 1, base + 2 * CR_MAX_NP, base + 3 * CR_MAX_NP);
+            if (!rc) rc = cr::pade_coefficients(freq, c0, np, 0, dr, 1, base + 4 * CR_MAX_NP, base + 5 * CR_MAX_NP);
+            status[k] = rc;
+        }
+    };
+    const int nthr = std::max(1, std::min<int>(nk / 16, (int)std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    for (int t = 1; t < nthr; ++t) th.emplace_back(work);
+    work();
+    for (auto& t : th) t.join();
+    for (int k = 0; k < nk; ++k)
+        if (status[k]) {
+            const auto& [freq, c0, np, ns, dr] = keys[k];
+            return e->fail(CR_EPADE, "Pade coefficients failed (freq=%g c0=%g np=%d ns=%d dr=%g): %s", freq,
+                           c0, np, ns, dr, status[k] == cr::kPadeNoConverge ? "Laguerre method not converging" : "bad arguments");
+        }
+    e->pd1.assign((size_t)b->n_rays * kSets * CR_MAX_NP, make_double2(0.0, 0.0));
+    e->pd2.assign((size_t)b->n_rays * kSets * CR_MAX_NP, make_double2(0.0, 0.0));
+    e->pd_n.assign((size_t)b->n_rays * kSets, 0);
+    for (int i = 0; i < b->n_rays; ++i) {
+        const int np = b->rays[i].np;
+        const cr::cd* base = res.data() + (size_t)ray_key[i] * 3 * 2 * CR_MAX_NP;
+        double2* p1 = e->pd1.data() + (size_t)i * kSets * CR_MAX_NP;
+        double2* p2 = e->pd2.data() + (size_t)i * kSets * CR_MAX_NP;
+        p1[0] = make_double2(0.0, 0.0);
+        p2[0] = make_double2(-1.0, 0.0);
+        e->pd_n[i * kSets + 0] = 1;
+        for (int s = 1; s < kSets; ++s) {
+            const cr::cd* a1 = base + (size_t)(s - 1) * 2 * CR_MAX_NP;
+            const cr::cd* a2 = a1 + CR_MAX_NP;
+            for (int j = 0; j < np; ++j) {
+                p1[s * CR_MAX_NP + j] = make_double2(a1[j].re, a1[j].im);
+                p2[s * CR_MAX_NP + j] = make_double2(a2[j].re, a2[j].im);
+            }
+            e->pd_n[i * kSets + s] = np;
+        }
+    }
+    return CR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int cr_abi_version(void) { return CR_ABI_VERSION; }
+
+int cr_global_error(char* buf, size_t len) {
+    if (!buf || len == 0) return CR_EINVAL;
+    snprintf(buf, len, "%s", g_error.c_str());
+    return CR_OK;
+}
+
+int cr_pade(double freq, double c0, int np, int ns, double dr, int ip, double* pd1, double* pd2) {
+    if (!pd1 || !pd2 || np < 1 || np > CR_MAX_NP || ns < 0 || ns > 2 || (ip != 1 && ip != 2)) {
+        set_global_error("cr_pade: invalid arguments (np=%d ns=%d ip=%d)", np, ns, ip);
+        return CR_EINVAL;
+    }
+    cr::cd a[CR_MAX_NP], b[CR_MAX_NP];
+    const int rc = cr::pade_coefficients(freq, c0, np, ns, dr, ip, a, b);
+    if (rc == cr::kPadeNoConverge) {
+        set_global_error("Laguerre method not converging");
+        return CR_EPADE;
+    }
+    if (rc) {
+        set_global_error("cr_pade: invalid arguments (freq=%g c0=%g)", freq, c0);
+        return CR_EINVAL;
+    }
+    for (int j = 0; j < np; ++j) {
+        pd1[2 * j] = a[j].re;
+        pd1[2 * j + 1] = a[j].im;
+        pd2[2 * j] = b[j].re;
+        pd2[2 * j + 1] = b[j].im;
+    }
+    return CR_OK;
+}
+
+int cr_create(const cr_batch* b, cr_engine** out) {
+    if (!out) {
+        set_global_error("cr_create: out is NULL");
+        return CR_EINVAL;
+    }
+    *out = nullptr;
+    const std::string msg = validate(b);
+    if (!msg.empty()) {
+        set_global_error("cr_create: %s", msg.c_str());
+        return CR_EINVAL;
+    }
+    cr_engine* e = new cr_engine();
+    e->n_rays = b->n_rays;
+    e->n_envs = b->n_envs;
+    e->precision = b->precision;
+    e->compute_grids = b->compute_grids;
+    e->line_len = b->line_len;
+    e->grid_len = b->compute_grids ? b->grid_len : 0;
+    e->pool_len = b->pool_len;
+    int rc = compute_pade_sets(e, b);
+    if (rc) {
+        set_global_error("%s", e->err.c_str());
+        delete e;
+        return rc;
+    }
+    // tiles: rays sorted by work, longest first, 32 per tile
+    std::vector<int> order(b->n_rays);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const double wx = (double)(b->rays[x].nz + 2) * (b->rays[x].nr + 3);
+        const double wy = (double)(b->rays[y].nz + 2) * (b->rays[y].nr + 3);
+        return wx > wy;
+    });
+    e->n_tiles = (b->n_rays + kTile - 1) / kTile;
+    e->tile_ray.assign((size_t)e->n_tiles * kTile, -1);
+    e->rays.resize(b->n_rays);
+    long long col = 0;
+    for (int t = 0; t < e->n_tiles; ++t) {
+        int rows = 0;
+        for (int l = 0; l < kTile; ++l) {
+            const int k = t * kTile + l;
+            if (k < b->n_rays) rows = std::max(rows, b->rays[order[k]].nz + 2);
+        }
+        for (int l = 0; l < kTile; ++l) {
+            const int k = t * kTile + l;
+            if (k >= b->n_rays) continue;
+            const int rid = order[k];
+            e->tile_ray[(size_t)t * kTile + l] = rid;
+            const cr_ray& r = b->rays[rid];
+            RayDev& d = e->rays[rid];
+            d.k0 = 2.0 * M_PI * r.freq / r.c0;
+            d.omega = 2.0 * M_PI * r.freq;
+            d.c0 = r.c0;
+            d.dz = r.dz;
+            d.dr = r.dr;
+            d.zmax = r.zmax;
+            d.lyrw_lambda = r.lyrw_lambda;
+            d.attnf = r.attnf;
+            d.rs = r.rs;
+            d.zs = r.zs;
+            d.zr = r.zr;
+            d.nz = r.nz;
+            d.nr = r.nr;
+            d.np = r.np;
+            d.ndr = r.ndr;
+            d.ndz = r.ndz;
+            d.nvr = r.nvr;
+            d.nvz = r.nvz;
+            d.env = r.env;
+            d.line_off = r.line_off;
+            d.grid_off = b->compute_grids ? r.grid_off : -1;
+            d.col = col + l;
+            e->point_updates += (double)r.nz * (double)r.nr;
+        }
+        col += (long long)rows * kTile;
+    }
+    e->col_elems = col;
+    e->envs.resize(b->n_envs);
+    for (int k = 0; k < b->n_envs; ++k) {
+        const cr_env& v = b->envs[k];
+        e->envs[k] = EnvDev{v.n_zss, v.n_rss, v.n_zsb, v.n_rsb, v.n_bt, 0, v.off};
+    }
+    e->pool.assign(b->pool, b->pool + b->pool_len);
+
+    cudaError_t ce = cudaGetDevice(&e->device);
+    if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+    for (auto& ev : e->ev)
+        if (ce == cudaSuccess) ce = cudaEventCreate(&ev);
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_rays, e->rays.size());
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_envs, e->envs.size());
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_pool, e->pool.size());
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tile_ray, e->tile_ray.size());
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_pd1, e->pd1.size());
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_pd2, e->pd2.size());
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_pd_n, e->pd_n.size());
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_f1, (size_t)col);
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_f2, (size_t)col);
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_f3, (size_t)col);
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_ksq, (size_t)col);
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_u, (size_t)col);
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_W, (size_t)col);
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_G, (size_t)col);
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tll, (size_t)e->line_len);
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_cpl, (size_t)e->line_len);
+    if (ce == cudaSuccess && e->compute_grids) ce = dev_alloc(e, &e->d_tlg, (size_t)e->grid_len);
+    if (ce == cudaSuccess && e->compute_grids) ce = dev_alloc(e, &e->d_cpg, (size_t)e->grid_len);
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_flags, (size_t)e->n_rays);
+    if (ce != cudaSuccess) {
+        set_global_error("cr_create: %s", cudaGetErrorString(ce));
+        const int code = ce == cudaErrorMemoryAllocation ? CR_ENOMEM : CR_ECUDA;
+        free_all(e);
+        delete e;
+        return code;
+    }
+    e->st.point_updates = e->point_updates;
+    e->st.tile_rays = kTile;
+    e->st.n_tiles = e->n_tiles;
+    e->st.device_bytes = e->device_bytes;
+    *out = e;
+    return CR_OK;
+}
+
+int cr_set_pade(cr_engine* e, int ray, int which, int n, const double* pd1, const double* pd2) {
+    if (!e) return CR_EINVAL;
+    if (ray < 0 || ray >= e->n_rays || which < 0 || which >= kSets || n < 1 || n > CR_MAX_NP || !pd1 || !pd2)
+        return e->fail(CR_EINVAL, "cr_set_pade: invalid arguments");
+    double2* p1 = e->pd1.data() + ((size_t)ray * kSets + which) * CR_MAX_NP;
+    double2* p2 = e->pd2.data() + ((size_t)ray * kSets + which) * CR_MAX_NP;
+    for (int j = 0; j < CR_MAX_NP; ++j) {
+        p1[j] = j < n ? make_double2(pd1[2 * j], pd1[2 * j + 1]) : make_double2(0.0, 0.0);
+        p2[j] = j < n ? make_double2(pd2[2 * j], pd2[2 * j + 1]) : make_double2(0.0, 0.0);
+    }
+    e->pd_n[(size_t)ray * kSets + which] = n;
+    e->uploaded = false;
+    return CR_OK;
+}
+
+int cr_upload(cr_engine* e) {
+    if (!e) return CR_EINVAL;
+    cudaError_t ce = cudaSetDevice(e->device);
+    float ms = 0.f;
+    if (ce == cudaSuccess) ce = cudaEventRecord(e->ev[0], e->stream);
+    auto cp = [&](void* dst, const void* src, size_t bytes) {
+        if (ce == cudaSuccess && bytes) ce = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, e->stream);
+    };
+    cp(e->d_rays, e->rays.data(), e->rays.size() * sizeof(RayDev));
+    cp(e->d_envs, e->envs.data(), e->envs.size() * sizeof(EnvDev));
+    cp(e->d_pool, e->pool.data(), e->pool.size() * sizeof(double));
+    cp(e->d_tile_ray, e->tile_ray.data(), e->tile_ray.size() * sizeof(int));
+    cp(e->d_pd1, e->pd1.data(), e->pd1.size() * sizeof(double2));
+    cp(e->d_pd2, e->pd2.data(), e->pd2.size() * sizeof(double2));
+    cp(e->d_pd_n, e->pd_n.data(), e->pd_n.size() * sizeof(int));
+    if (ce == cudaSuccess) ce = cudaEventRecord(e->ev[1], e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "cr_upload");
+    e->st.h2d_ms = ms;
+    e->st.h2d_bytes = (long long)(e->rays.size() * sizeof(RayDev) + e->envs.size() * sizeof(EnvDev) +
+                                  e->pool.size() * sizeof(double) + e->tile_ray.size() * sizeof(int) +
+                                  2 * e->pd1.size() * sizeof(double2) + e->pd_n.size() * sizeof(int));
+    e->uploaded = true;
+    return CR_OK;
+}
+
+int cr_march(cr_engine* e) {
+    if (!e) return CR_EINVAL;
+    if (!e->uploaded) return e->fail(CR_ESTATE, "cr_march: call cr_upload first");
+    cudaError_t ce = cudaSetDevice(e->device);
+    MarchArgs a;
+    a.rays = e->d_rays;
+    a.tile_ray = e->d_tile_ray;
+    a.envs = e->d_envs;
+    a.pool = e->d_pool;
+    a.pd1 = e->d_pd1;
+    a.pd2 = e->d_pd2;
+    a.pd_n = e->d_pd_n;
+    a.f1 = e->d_f1;
+    a.f2 = e->d_f2;
+    a.f3 = e->d_f3;
+    a.ksq = e->d_ksq;
+    a.u = e->d_u;
+    a.W = e->d_W;
+    a.G = e->d_G;
+    a.tll = e->d_tll;
+    a.cpl = e->d_cpl;
+    a.tlg = e->d_tlg;
+    a.cpg = e->d_cpg;
+    a.flags = e->d_flags;
+    a.compute_grids = e->compute_grids;
+    float ms = 0.f;
+    if (ce == cudaSuccess) ce = cudaEventRecord(e->ev[0], e->stream);
+    if (ce == cudaSuccess) {
+        march_kernel<<<e->n_tiles, kTile, 0, e->stream>>>(a);
+        ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cudaEventRecord(e->ev[1], e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "cr_march");
+    e->st.march_ms = ms;
+    e->st.kernel_launches = 1;
+    std::vector<int> fl(e->n_rays);
+    ce = cudaMemcpy(fl.data(), e->d_flags, fl.size() * sizeof(int), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "cr_march (flags)");
+    int failed = 0;
+    for (int v : fl) failed += (v != 0);
+    e->st.rays_failed = failed;
+    e->marched = true;
+    if (failed) return e->fail(CR_ENAN, "%d ray(s) produced a non-finite field", failed);
+    return CR_OK;
+}
+
+int cr_download(cr_engine* e, const cr_outputs* out) {
+    if (!e) return CR_EINVAL;
+    if (!out || !out->tll || !out->cpl) return e->fail(CR_EINVAL, "cr_download: tll and cpl are required");
+    if (!e->marched) return e->fail(CR_ESTATE, "cr_download: nothing marched yet");
+    cudaError_t ce = cudaSetDevice(e->device);
+    float ms = 0.f;
+    long long bytes = 0;
+    if (ce == cudaSuccess) ce = cudaEventRecord(e->ev[2], e->stream);
+    auto cp = [&](void* dst, const void* src, size_t n) {
+        if (ce == cudaSuccess && n && dst) {
+            ce = cudaMemcpyAsync(dst, src, n, cudaMemcpyDeviceToHost, e->stream);
+            bytes += (long long)n;
+        }
+    };
+    cp(out->tll, e->d_tll, (size_t)e->line_len * sizeof(double));
+    cp(out->cpl, e->d_cpl, (size_t)e->line_len * sizeof(double2));
+    if (e->compute_grids) {
+        cp(out->tlg, e->d_tlg, (size_t)e->grid_len * sizeof(double));
+        cp(out->cpg, e->d_cpg, (size_t)e->grid_len * sizeof(double2));
+    }
+    if (ce == cudaSuccess) ce = cudaEventRecord(e->ev[3], e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e->ev[2], e->ev[3]);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "cr_download");
+    e->st.d2h_ms = ms;
+    e->st.d2h_bytes = bytes;
+    return CR_OK;
+}
+
+int cr_run(cr_engine* e, const cr_outputs* out) {
+    int rc = cr_upload(e);
+    if (rc) return rc;
+    rc = cr_march(e);
+    if (rc) return rc;
+    return cr_download(e, out);
+}
+
+int cr_ray_flags(cr_engine* e, int32_t* flags, int n) {
+    if (!e || !flags || n < e->n_rays) return CR_EINVAL;
+    cudaError_t ce = cudaMemcpy(flags, e->d_flags, (size_t)e->n_rays * sizeof(int), cudaMemcpyDeviceToHost);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "cr_ray_flags");
+    return CR_OK;
+}
+
+int cr_get_stats(const cr_engine* e, cr_stats* st) {
+    if (!e || !st) return CR_EINVAL;
+    *st = e->st;
+    return CR_OK;
+}
+
+int cr_last_error(const cr_engine* e, char* buf, size_t len) {
+    if (!e || !buf || len == 0) return CR_EINVAL;
+    snprintf(buf, len, "%s", e->err.c_str());
+    return CR_OK;
+}
+
+void cr_destroy(cr_engine* e) {
+    if (!e) return;
+    cudaSetDevice(e->device);
+    if (e->stream) cudaStreamSynchronize(e->stream);
+    free_all(e);
+    delete e;
+}
+
+}  // extern "C"

@@ -1,0 +1,118 @@
+"""Python handle on one native engine (cr_engine) and its host buffers."""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .batch import Batch
+
+
+class Engine:
+    """Owns a cr_engine built from a packed :class:`Batch`.
+
+    ``run()`` is the full device march with host outputs.  ``upload`` /
+    ``march`` / ``download`` expose the three phases separately (the bench
+    times ``march`` alone with inputs resident, and ``run`` end to end).
+    Output buffers may be supplied by the caller (e.g. pinned memory); they
+    must be C-contiguous float64 (tll, tlg) and complex128 (cpl, cpg).
+    """
+
+    def __init__(self, batch: Batch, precision="plain"):
+        self.lib = _lib.load()
+        self.batch = batch
+        prec = {"plain": _lib.CR_PLAIN_C128, "chosen": _lib.CR_CHOSEN_C64R}.get(precision)
+        if prec is None:
+            raise ValueError(f"precision must be 'plain' or 'chosen', got {precision!r}")
+        self._keep = (np.ascontiguousarray(batch.rays), np.ascontiguousarray(batch.envs),
+                      np.ascontiguousarray(batch.pool, dtype=np.float64))
+        rays, envs, pool = self._keep
+        desc = _lib.CrBatch()
+        desc.n_rays = len(rays)
+        desc.n_envs = len(envs)
+        desc.rays = rays.ctypes.data
+        desc.envs = envs.ctypes.data
+        desc.pool = pool.ctypes.data
+        desc.pool_len = pool.size
+        desc.precision = prec
+        desc.compute_grids = 1 if batch.compute_grids else 0
+        desc.line_len = batch.line_len
+        desc.grid_len = batch.grid_len
+        handle = ctypes.c_void_p()
+        _lib.check(self.lib.cr_create(ctypes.byref(desc), ctypes.byref(handle)))
+        self.handle = handle
+
+    # -- phases -------------------------------------------------------------
+    def upload(self):
+        _lib.check(self.lib.cr_upload(self.handle), self.handle)
+
+    def march(self):
+        _lib.check(self.lib.cr_march(self.handle), self.handle)
+
+    def alloc_outputs(self):
+        b = self.batch
+        out = {"tll": np.empty(max(b.line_len, 1), np.float64),
+               "cpl": np.empty(max(b.line_len, 1), np.complex128)}
+        if b.compute_grids:
+            out["tlg"] = np.empty(max(b.grid_len, 1), np.float64)
+            out["cpg"] = np.empty(max(b.grid_len, 1), np.complex128)
+        return out
+
+    def _outputs_struct(self, out):
+        o = _lib.CrOutputs()
+        for name, dt in (("tll", np.float64), ("cpl", np.complex128), ("tlg", np.float64),
+                         ("cpg", np.complex128)):
+            a = out.get(name)
+            if a is None:
+                setattr(o, name, None)
+                continue
+            if isinstance(a, np.ndarray):
+                if a.dtype != dt or not a.flags.c_contiguous:
+                    raise ValueError(f"{name} must be C-contiguous {np.dtype(dt).name}")
+                setattr(o, name, a.ctypes.data)
+            else:  # an object exposing a raw pointer (e.g. a pinned torch tensor)
+                setattr(o, name, int(a.data_ptr()))
+        return o
+
+    def download(self, out):
+        o = self._outputs_struct(out)
+        _lib.check(self.lib.cr_download(self.handle, ctypes.byref(o)), self.handle)
+        return out
+
+    def run(self, out=None):
+        out = out if out is not None else self.alloc_outputs()
+        o = self._outputs_struct(out)
+        _lib.check(self.lib.cr_run(self.handle, ctypes.byref(o)), self.handle)
+        return out
+
+    def set_pade(self, ray, which, pd1, pd2):
+        p1 = np.ascontiguousarray(pd1, dtype=np.complex128)
+        p2 = np.ascontiguousarray(pd2, dtype=np.complex128)
+        _lib.check(self.lib.cr_set_pade(self.handle, ray, which, p1.size, p1.ctypes.data,
+                                        p2.ctypes.data), self.handle)
+
+    def ray_flags(self):
+        f = np.zeros(self.batch.n_rays, np.int32)
+        _lib.check(self.lib.cr_ray_flags(self.handle, f.ctypes.data, f.size), self.handle)
+        return f
+
+    def stats(self):
+        st = _lib.CrStats()
+        _lib.check(self.lib.cr_get_stats(self.handle, ctypes.byref(st)), self.handle)
+        return {k: getattr(st, k) for k, _ in st._fields_}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.cr_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,190 @@
+/*
+ * cupyram_b200.h - C ABI of the B200 split-step Pade parabolic-equation engine.
+ *
+ * The engine replaces the range march of clapeyre/cupyram (CuPyRAM.run):
+ * profile interpolation, range-index updates, Galerkin assembly, the np
+ * Pade tridiagonal sweeps per range step, the self-starter and the
+ * receiver / TL-grid extraction.  Everything here is plain C: host pointers,
+ * sizes and int status codes; no CUDA or torch types cross the boundary, so
+ * ctypes, cffi or any C FFI can bind it.
+ *
+ * Units: metres, seconds, Hz, m/s, g/cm^3, dB/wavelength.  Complex numbers are
+ * stored as interleaved (re, im) float64 pairs.
+ *
+ * Threading: one engine per host thread.  Each engine owns a CUDA stream on
+ * the device that was current when it was created.  The library never calls
+ * exit() or abort(); every failure is reported by a status code and the text
+ * from cr_last_error().
+ */
+#ifndef CUPYRAM_B200_H
+#define CUPYRAM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CR_ABI_VERSION 1
+/* Largest number of Pade terms a ray may use. */
+#define CR_MAX_NP 10
+
+/* Status codes returned by every entry point. */
+enum cr_status {
+    CR_OK = 0,
+    CR_EINVAL = 1,    /* invalid argument or inconsistent batch description */
+    CR_ECUDA = 2,     /* CUDA runtime error (text in cr_last_error)          */
+    CR_EPADE = 3,     /* Pade root finding did not converge                   */
+    CR_ETIMEOUT = 4,  /* a device-side iteration cap was hit                  */
+    CR_ENAN = 5,      /* a ray produced a non-finite field (see cr_ray_flags) */
+    CR_ENOMEM = 6,    /* device or host allocation failed                     */
+    CR_ESTATE = 7     /* call made in the wrong order (e.g. march before upload) */
+};
+
+/* Arithmetic form of the range march. */
+enum cr_precision {
+    CR_PLAIN_C128 = 0,   /* complex128 field and sweeps, FP64 arithmetic          */
+    CR_CHOSEN_C64R = 1   /* complex64 sweeps, FP32 accumulation, one FP64-residual
+                            refinement step per Pade term; field kept in complex128 */
+};
+
+/*
+ * One ray (one "calculation" of the reference: an environment at one
+ * frequency).  The grid and step sizes are per ray; the reference's shared
+ * grid is the special case where all rays carry the same values.
+ * Mirrors the per-calculation state of CuPyRAM.setup (cupyram/cupyram.py:528-726).
+ */
+typedef struct cr_ray {
+    double freq;         /* Hz                                                  */
+    double c0;           /* reference sound speed (m/s); k0 = 2*pi*freq/c0      */
+    double zs, zr;       /* source / receiver depth (m)                         */
+    double dz, dr;       /* depth and range step (m)                            */
+    double zmax;         /* bottom of the computational grid incl. the layer (m) */
+    double lyrw_lambda;  /* absorbing-layer width in metres (lyrw * lambda)     */
+    double attnf;        /* attenuation at the bottom of the layer (dB/wavelength, 10 in RAM) */
+    double rs;           /* range beyond which the stability constraints are dropped (m) */
+    int32_t nz;          /* interior depth points; the grid has nz+2 rows       */
+    int32_t nr;          /* march steps after the self-starter                  */
+    int32_t np;          /* Pade terms, 1..CR_MAX_NP                            */
+    int32_t ns;          /* stability constraints 0..2                          */
+    int32_t ndr, ndz;    /* output decimation in range / depth                  */
+    int32_t nvr, nvz;    /* output ranges / output depths (TL grid rows)        */
+    int32_t env;         /* index into the environment table                    */
+    int32_t reserved;
+    int64_t line_off;    /* element offset of this ray's TL line in tll / cpl   */
+    int64_t grid_off;    /* element offset of this ray's [nvz][nvr] grid, or -1 */
+} cr_ray;
+
+/*
+ * One environment record.  Its arrays live contiguously in the float64 pool
+ * starting at `off`, in this order:
+ *   z_ss[n_zss], rp_ss[n_rss], cw[n_rss][n_zss],
+ *   z_sb[n_zsb] (absolute depths), rp_sb[n_rsb],
+ *   cb[n_rsb][n_zsb], rhob[n_rsb][n_zsb], attn[n_rsb][n_zsb],
+ *   rb[n_bt], zb[n_bt]   (bathymetry ranges and depths, extended to rmax)
+ * Profiles are stored profile-major (one contiguous depth profile per update
+ * range), the transpose of the reference's cw[depth, range] input.
+ */
+typedef struct cr_env {
+    int32_t n_zss, n_rss, n_zsb, n_rsb, n_bt, reserved;
+    int64_t off;
+} cr_env;
+
+typedef struct cr_batch {
+    int32_t n_rays, n_envs;
+    const cr_ray* rays;
+    const cr_env* envs;
+    const double* pool;
+    int64_t pool_len;
+    int32_t precision;      /* enum cr_precision                                */
+    int32_t compute_grids;  /* 0: TL line only; 1: also TL / CP grids           */
+    int64_t line_len;       /* total elements of tll (and of cpl, complex)      */
+    int64_t grid_len;       /* total elements of tlg (and of cpg, complex)      */
+} cr_batch;
+
+/* Caller-owned host output buffers (cpl, cpg interleaved complex). */
+typedef struct cr_outputs {
+    double* tll;   /* [line_len]                  TL line (dB)          */
+    double* cpl;   /* [2*line_len]                complex pressure line */
+    double* tlg;   /* [grid_len] or NULL          TL grid (dB)          */
+    double* cpg;   /* [2*grid_len] or NULL        complex pressure grid */
+} cr_outputs;
+
+/* Timing and work counters of the last march (device clock). */
+typedef struct cr_stats {
+    double march_ms;          /* self-starter + range march, CUDA events        */
+    double assemble_ms;       /* initial profile assembly                       */
+    double h2d_ms, d2h_ms;    /* last upload / download                         */
+    double point_updates;     /* sum over rays of nz * nr                       */
+    int64_t h2d_bytes, d2h_bytes;
+    int32_t kernel_launches;  /* kernels launched by the last cr_march           */
+    int32_t rays_failed;      /* rays whose field went non-finite               */
+    int32_t tile_rays;        /* rays per tile in the device layout             */
+    int32_t n_tiles;
+    int64_t device_bytes;     /* device memory held by the engine               */
+} cr_stats;
+
+typedef struct cr_engine cr_engine;
+
+/* ABI version of the loaded library (CR_ABI_VERSION). */
+int cr_abi_version(void);
+
+/*
+ * Pade coefficients of exp(i*k0*dr*(sqrt(1+X)-1)) (ip=1) or of the
+ * self-starter operator (ip=2), product form, FP64.
+ * Replaces cupyram/pade.py:324-417 compute_pade_coefficients(freq, c0,
+ * np_pade, ns, dr, ip).  pd1, pd2: 2*np doubles each (re, im interleaved).
+ * Returns CR_EPADE when Laguerre iteration fails to converge
+ * (cupyram/pade.py:290-291 raises ValueError there).
+ */
+int cr_pade(double freq, double c0, int np, int ns, double dr, int ip,
+            double* pd1, double* pd2);
+
+/*
+ * Build an engine for a batch: validates the description, computes the Pade
+ * sets of every ray (self-starter, march, march without stability
+ * constraints) on the host in FP64, sorts rays into device tiles by work and
+ * allocates device memory.  Replaces the set-up half of CuPyRAM.run
+ * (cupyram/cupyram.py:528-726: setup, profl, Pade batch).
+ */
+int cr_create(const cr_batch* batch, cr_engine** out);
+
+/* Copy the batch's environments and per-ray parameters to the device. */
+int cr_upload(cr_engine* e);
+
+/*
+ * Self-starter + full range march on the device, inputs already resident.
+ * Replaces the loop of CuPyRAM.run (cupyram/cupyram.py:296-317: updat,
+ * _propagate_step, _outpt) and CuPyRAM.selfs (:1001-1063).  Synchronous.
+ */
+int cr_march(cr_engine* e);
+
+/* Copy outputs to the caller's host buffers (layout given by line_off/grid_off). */
+int cr_download(cr_engine* e, const cr_outputs* out);
+
+/* cr_upload + cr_march + cr_download: the whole CuPyRAM.run on the device. */
+int cr_run(cr_engine* e, const cr_outputs* out);
+
+/* Override one ray's Pade set: which = 0 self-starter (1-X)^-2 factor,
+ * 1 self-starter ip=2, 2 march, 3 march after rs.  n terms (<= CR_MAX_NP). */
+int cr_set_pade(cr_engine* e, int ray, int which, int n, const double* pd1, const double* pd2);
+
+/* Per-ray status flags of the last march (bit 0: non-finite field). */
+int cr_ray_flags(cr_engine* e, int32_t* flags, int n);
+
+int cr_get_stats(const cr_engine* e, cr_stats* st);
+
+/* Copy the last error message (NUL-terminated, truncated to len). */
+int cr_last_error(const cr_engine* e, char* buf, size_t len);
+
+/* Message of the last failure of a call that had no engine (cr_create, cr_pade). */
+int cr_global_error(char* buf, size_t len);
+
+void cr_destroy(cr_engine* e);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUPYRAM_B200_H */

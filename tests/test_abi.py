@@ -1,0 +1,105 @@
+"""The C ABI library: loads, exports every declared symbol, host-only entry points.
+
+No compute call here touches a GPU: cr_pade is host code, and cr_create
+rejects invalid batches before any CUDA call.
+"""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from cupyram_b200 import _lib, compute_pade_coefficients
+from golden_cases import GOLDEN, load_case
+from cupyram_b200 import batch as B
+
+HEADERS = sorted((Path(__file__).resolve().parent.parent / "include").glob("*.h"))
+
+
+def declared_symbols():
+    syms = set()
+    for h in HEADERS:
+        text = h.read_text()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^\s*(?:[A-Za-z_][\w\s\*]*?)\b(cr_\w+)\s*\(", text, flags=re.M):
+            syms.add(m.group(1))
+    return syms
+
+
+def test_headers_declare_entry_points():
+    syms = declared_symbols()
+    for s in ("cr_create", "cr_run", "cr_march", "cr_pade", "cr_destroy", "cr_last_error"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol(lib_built):
+    lib = ctypes.CDLL(str(lib_built))
+    missing = [s for s in sorted(declared_symbols()) if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_abi_version(lib_built):
+    assert _lib.load().cr_abi_version() == _lib.ABI_VERSION
+
+
+def test_struct_layouts_match_header(lib_built):
+    # sizes implied by the header's field lists
+    assert _lib.RAY_DTYPE.itemsize == 136
+    assert _lib.ENV_DTYPE.itemsize == 32
+    assert ctypes.sizeof(_lib.CrBatch) == 64
+    assert ctypes.sizeof(_lib.CrOutputs) == 32
+
+
+def test_pade_matches_reference(lib_built):
+    d = np.load(GOLDEN / "pade_ref.npz")
+    worst = 0.0
+    for row, p1, p2 in zip(d["params"], d["pd1"], d["pd2"]):
+        np_, ns, ip, freq, dr, c0 = row
+        a, c = compute_pade_coefficients(freq, c0, int(np_), ns=int(ns), dr=dr, ip=int(ip))
+        n = int(np_)
+        worst = max(worst, np.max(np.abs(a - p1[:n])), np.max(np.abs(c - p2[:n])))
+    assert worst < 1e-8, worst
+
+
+def test_pade_bad_arguments(lib_built):
+    with pytest.raises(ValueError):
+        compute_pade_coefficients(50.0, 1500.0, 0)
+    with pytest.raises(ValueError):
+        compute_pade_coefficients(50.0, 1500.0, 11)
+    with pytest.raises(ValueError):
+        compute_pade_coefficients(-50.0, 1500.0, 4)
+
+
+def _desc(b, **over):
+    rays = np.ascontiguousarray(b.rays.copy())
+    for k, v in over.items():
+        rays[k] = v
+    d = _lib.CrBatch()
+    d.n_rays, d.n_envs = len(rays), len(b.envs)
+    d.rays, d.envs, d.pool = rays.ctypes.data, b.envs.ctypes.data, b.pool.ctypes.data
+    d.pool_len, d.precision, d.compute_grids = b.pool.size, 0, 1
+    d.line_len, d.grid_len = b.line_len, b.grid_len
+    return d, rays
+
+
+@pytest.mark.parametrize("field,value", [("np", 0), ("np", 11), ("ns", 3), ("nz", 1), ("dz", 0.0),
+                                         ("env", 5), ("ndr", 0), ("line_off", 10**9), ("zs", 1e9)])
+def test_create_rejects_invalid_batch(lib_built, field, value):
+    args, kw, _ = load_case("pekeris_small")
+    envs, p, zs, zr, pr = B.prepare(*args, dict(kw))
+    b = B.build_batch(envs, p, zs, zr, pr, True)
+    d, keep = _desc(b, **{field: value})
+    h = ctypes.c_void_p()
+    rc = _lib.load().cr_create(ctypes.byref(d), ctypes.byref(h))
+    assert rc == _lib.CR_EINVAL
+    assert not h.value
+    assert _lib.global_error()
+
+
+def test_null_arguments(lib_built):
+    lib = _lib.load()
+    assert lib.cr_create(None, None) == _lib.CR_EINVAL
+    assert lib.cr_upload(None) == _lib.CR_EINVAL
+    assert lib.cr_march(None) == _lib.CR_EINVAL
+    lib.cr_destroy(None)

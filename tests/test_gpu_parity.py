@@ -1,0 +1,78 @@
+"""Parity of the sm_100a engine (through the C ABI) with the oracle and the reference.
+
+Tolerances (dB of transmission loss):
+* engine vs the oracle's plain complex128 form on the same inputs: 1e-3 dB on
+  the TL line (the engine eliminates every other Pade term upwards, so the two
+  differ only by rounding);
+* engine vs the reference's own outputs (tests/golden): 0.01 dB max on the TL
+  line - the reference's own parity bar against PyRAM (tests/test_utils.py:30-37);
+* RAM v1.5 Fortran line: mean 0.01 dB (tests/test_reference.py:28,192).
+"""
+import numpy as np
+import pytest
+
+from golden_cases import CASES, GOLDEN, load_case
+from cupyram_b200 import CuPyRAM
+from cupyram_b200 import batch as B
+from cupyram_b200.engine import Engine
+from oracle import oracle
+
+pytestmark = pytest.mark.gpu
+
+TOL_ORACLE = 1e-3
+TOL_REF = 0.01
+
+
+def _batch(name, grids=True):
+    args, kw, fx = load_case(name)
+    envs, p, zs, zr, pr = B.prepare(*args, dict(kw))
+    return B.build_batch(envs, p, zs, zr, pr, grids), fx
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_engine_vs_oracle(cuda_device, name):
+    b, _ = _batch(name)
+    with Engine(b) as eng:
+        out = eng.run()
+        assert eng.stats()["rays_failed"] == 0
+    ref = oracle.run(b, "plain")
+    n = b.line_len
+    d = np.abs(out["tll"][:n] - ref["tll"][:n])
+    assert d.max() < TOL_ORACLE, d.max()
+    cp = np.abs(out["cpl"][:n] - ref["cpl"][:n]).max() / np.abs(ref["cpl"][:n]).max()
+    assert cp < 1e-6, cp
+    g = np.abs(out["tlg"][:b.grid_len] - ref["tlg"][:b.grid_len])
+    assert np.percentile(g, 99.9) < TOL_ORACLE
+    gc = np.abs(out["cpg"][:b.grid_len] - ref["cpg"][:b.grid_len]).max() / np.abs(ref["cpg"][:b.grid_len]).max()
+    assert gc < 1e-6, gc
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_cupyram_vs_reference(cuda_device, name):
+    args, kw, fx = load_case(name)
+    res = CuPyRAM(*args, **kw).run()
+    tl = np.asarray(res["TL Line"])
+    assert tl.shape == fx["tl_line"].shape
+    assert np.array_equal(res["Ranges"], fx["ranges"])
+    assert np.allclose(res["Depths"], fx["depths"])
+    d = np.abs(tl - fx["tl_line"])
+    assert d.max() <= TOL_REF, d.max()
+    grid = np.asarray(res["TL Grid"])
+    assert grid.shape == fx["tl_grid"].shape
+    dg = np.abs(grid - fx["tl_grid"])
+    assert np.percentile(dg, 99) <= TOL_REF and dg.max() <= 0.05
+
+
+def test_ram_v15_vs_fortran(cuda_device):
+    args, kw, _ = load_case("ram_v15")
+    res = CuPyRAM(*args, **kw).run()
+    f = np.load(GOLDEN / "ram_v15_fortran.npz")
+    assert np.array_equal(res["Ranges"], f["ranges"])
+    assert np.mean(np.abs(res["TL Line"] - f["tl"])) <= 0.01
+
+
+def test_no_grid_still_computes_line(cuda_device):
+    args, kw, fx = load_case("pekeris_small")
+    res = CuPyRAM(*args, compute_grids=False, **kw).run()
+    assert res["TL Grid"] is None and res["CP Grid"] is None
+    assert np.abs(res["TL Line"] - fx["tl_line"]).max() <= TOL_REF

@@ -1,0 +1,106 @@
+"""The CPU oracle, pinned against the reference's own outputs.
+
+* tests/golden/<case>.npz - the unmodified reference (clapeyre/cupyram) run on
+  CPU under Numba's CUDA simulator by tests/golden/make_golden.py;
+* tests/golden/ram_v15_fortran.npz - RAM v1.5's Fortran TL line (the
+  reference's tests/tl_ref.line), pinned by the reference at mean |dTL| <= 0.01 dB
+  (tests/test_reference.py:28,192);
+* tests/golden/pade_ref.npz - the reference's pade.py, pinned at abs 1e-8
+  (tests/test_pade_coefficients.py:23).
+"""
+import numpy as np
+import pytest
+
+from golden_cases import CASES, GOLDEN, load_case
+from cupyram_b200 import batch as B
+from oracle import oracle
+
+# dB tolerances on the TL line (plain engine vs the reference: 0.01 dB)
+TOL_LINE = 0.01
+# simulator-promotion mode reproduces the fixtures at rounding level
+TOL_SIM = 1e-3
+
+
+def _prep(name, compute_grids=True):
+    args, kw, fx = load_case(name)
+    envs, p, zs, zr, per_ray = B.prepare(*args, dict(kw))
+    b = B.build_batch(envs, p, zs, zr, per_ray, compute_grids)
+    return b, fx
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_grid_matches_reference(name):
+    b, fx = _prep(name)
+    assert int(b.nz[0]) == int(fx["nz"])
+    assert b.zmax[0] == pytest.approx(float(fx["zmax"]), rel=1e-12)
+    assert np.array_equal(b.vr[0], fx["ranges"])
+    assert np.allclose(b.vz[0], fx["depths"])
+
+
+@pytest.mark.parametrize("mode", ["sim", "ref", "plain", "f64"])
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_tl_line_vs_reference(name, mode):
+    b, fx = _prep(name)
+    out = oracle.run(b, mode)
+    n, nvr = b.n_rays, int(b.nvr[0])
+    tl = out["tll"][: n * nvr].reshape(fx["tl_line"].shape)
+    d = np.abs(tl - fx["tl_line"])
+    assert np.all(np.isfinite(tl))
+    assert d.max() <= (TOL_SIM if mode == "sim" else TOL_LINE), d.max()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_cp_line_vs_reference(name):
+    b, fx = _prep(name)
+    out = oracle.run(b, "sim")
+    n, nvr = b.n_rays, int(b.nvr[0])
+    cp = out["cpl"][: n * nvr].reshape(fx["cp_line"].shape)
+    rel = np.max(np.abs(cp - fx["cp_line"])) / np.max(np.abs(fx["cp_line"]))
+    assert rel < 1e-5, rel
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_tl_grid_vs_reference(name):
+    b, fx = _prep(name)
+    out = oracle.run(b, "plain")
+    n, nvr, nvz = b.n_rays, int(b.nvr[0]), int(b.nvz[0])
+    tg = out["tlg"][: n * nvz * nvr].reshape(fx["tl_grid"].shape)
+    d = np.abs(tg - fx["tl_grid"])
+    # grid cells include interference nulls, where dTL amplifies rounding:
+    # the bulk is held to 0.01 dB, every cell to 0.05 dB
+    assert np.percentile(d, 99) <= TOL_LINE
+    assert d.max() <= 0.05
+
+
+@pytest.mark.parametrize("mode", ["ref", "plain", "f64"])
+def test_oracle_vs_ram_fortran(mode):
+    """RAM v1.5 test case against the Fortran output (mean |dTL| <= 0.01 dB)."""
+    b, _ = _prep("ram_v15")
+    f = np.load(GOLDEN / "ram_v15_fortran.npz")
+    assert np.array_equal(b.vr[0], f["ranges"])
+    out = oracle.run(b, mode)
+    tl = out["tll"][: int(b.nvr[0])]
+    d = np.abs(tl - f["tl"])
+    assert d.mean() <= 0.01, d.mean()
+
+
+def test_oracle_pade_vs_reference():
+    d = np.load(GOLDEN / "pade_ref.npz")
+    worst = 0.0
+    for row, p1, p2 in zip(d["params"], d["pd1"], d["pd2"]):
+        np_, ns, ip, freq, dr, c0 = row
+        a, c = oracle.pade(freq, c0, int(np_), int(ns), dr, int(ip))
+        n = int(np_)
+        worst = max(worst, np.max(np.abs(a - p1[:n])), np.max(np.abs(c - p2[:n])))
+    assert worst < 1e-8, worst
+
+
+def test_oracle_batch_rays_independent():
+    """A ray's result does not depend on the other rays of its batch."""
+    b, _ = _prep("ragged_batch")
+    full = oracle.run(b, "plain")
+    for k in range(b.n_rays):
+        one = oracle.run(b, "plain", rays=[k])
+        lo, n = int(b.rays["line_off"][k]), int(b.rays["nvr"][k])
+        # the single-ray run starts its line at the ray's own offset
+        assert np.array_equal(one["tll"][lo:lo + n], full["tll"][lo:lo + n])
