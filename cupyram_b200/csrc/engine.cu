@@ -1151,3 +1151,261 @@ void cr_destroy(cr_engine* e) {
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// cr_march_static: the march without any allocation.
+//
+// For callers that cannot allocate device memory when they need a march (a
+// real-time loop that forbids allocation after start-up, or a plug-in whose
+// host application owns all device memory through its own pool).  Everything
+// the march needs besides the caller's inputs and outputs lives in one
+// file-scope device array of CR_STATIC_SCRATCH_BYTES; the per-ray tables and
+// the Pade sets are built on the device from the raw cr_ray records, so the
+// host side needs no heap either.
+// ===========================================================================
+namespace {
+
+__device__ __align__(256) unsigned char g_static_scratch[CR_STATIC_SCRATCH_BYTES];
+
+static_assert(sizeof(cr_env) == sizeof(EnvDev), "cr_env and EnvDev must share a layout");
+static_assert(sizeof(cr_ray) == 136, "cr_ray layout changed");
+
+// Device address of g_static_scratch per device, looked up on the first call
+// on that device (host code cannot use the symbol's name as an address).
+constexpr int kMaxDevices = 64;
+void* g_static_ptr[kMaxDevices] = {};
+std::mutex g_static_mu;
+
+int static_scratch_ptr(int dev, void** out) {
+    if (dev < 0 || dev >= kMaxDevices) return CR_EINVAL;
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t ce = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (ce != cudaSuccess || !p) {
+            set_global_error("cr_march_static: cudaGetSymbolAddress failed: %s", cudaGetErrorString(ce));
+            return CR_ECUDA;
+        }
+        g_static_ptr[dev] = p;
+    }
+    *out = g_static_ptr[dev];
+    return CR_OK;
+}
+
+struct StaticLayout {
+    size_t rays_raw, envs, pool, rays, tile_ray, pd1, pd2, pd_n, flags, status, f1, f2, f3, ksq, u, W, G;
+    size_t total;
+    long long col_elems;
+    int n_tiles, rows;
+};
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+void static_layout(const cr_batch* b, StaticLayout* L) {
+    int rows = 0;
+    for (int i = 0; i < b->n_rays; ++i) rows = std::max(rows, b->rays[i].nz + 2);
+    L->rows = rows;
+    L->n_tiles = (b->n_rays + kTile - 1) / kTile;
+    L->col_elems = (long long)L->n_tiles * rows * kTile;
+    size_t o = 0;
+    auto take = [&](size_t bytes) {
+        const size_t at = o;
+        o = align256(o + bytes);
+        return at;
+    };
+    const size_t nr = (size_t)b->n_rays;
+    L->rays_raw = take(nr * sizeof(cr_ray));
+    L->envs = take((size_t)b->n_envs * sizeof(cr_env));
+    L->pool = take((size_t)b->pool_len * sizeof(double));
+    L->rays = take(nr * sizeof(RayDev));
+    L->tile_ray = take((size_t)L->n_tiles * kTile * sizeof(int));
+    L->pd1 = take(nr * kSets * CR_MAX_NP * sizeof(double2));
+    L->pd2 = take(nr * kSets * CR_MAX_NP * sizeof(double2));
+    L->pd_n = take(nr * kSets * sizeof(int));
+    L->flags = take(nr * sizeof(int));
+    L->status = take(sizeof(int));
+    const size_t ce = (size_t)L->col_elems;
+    L->f1 = take(ce * sizeof(float));
+    L->f2 = take(ce * sizeof(float));
+    L->f3 = take(ce * sizeof(float));
+    L->ksq = take(ce * sizeof(float2));
+    L->u = take(ce * sizeof(double2));
+    L->W = take(ce * sizeof(double2));
+    L->G = take(ce * sizeof(double2));
+    L->total = o;
+}
+
+// One thread per tile slot: derive RayDev, the tile map and the Pade sets of
+// one ray (device FP64 Pade, same code as the host path).  Bit 0 of *status:
+// a Pade set failed.
+__global__ void static_setup_kernel(const cr_ray* raw, int n_rays, int compute_grids, int rows, RayDev* rays,
+                                    int* tile_ray, double2* pd1, double2* pd2, int* pd_n, int* flags, int* status,
+                                    int n_slots) {
+    const int b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b == 0) *status = 0;
+    if (b >= n_slots) return;
+    if (b >= n_rays) {
+        tile_ray[b] = -1;
+        return;
+    }
+    tile_ray[b] = b;
+    const cr_ray r = raw[b];
+    RayDev d;
+    d.k0 = 2.0 * M_PI * r.freq / r.c0;
+    d.omega = 2.0 * M_PI * r.freq;
+    d.c0 = r.c0;
+    d.dz = r.dz;
+    d.dr = r.dr;
+    d.zmax = r.zmax;
+    d.lyrw_lambda = r.lyrw_lambda;
+    d.attnf = r.attnf;
+    d.rs = r.rs;
+    d.zs = r.zs;
+    d.zr = r.zr;
+    d.nz = r.nz;
+    d.nr = r.nr;
+    d.np = r.np;
+    d.ndr = r.ndr;
+    d.ndz = r.ndz;
+    d.nvr = r.nvr;
+    d.nvz = r.nvz;
+    d.env = r.env;
+    d.line_off = r.line_off;
+    d.grid_off = compute_grids ? r.grid_off : -1;
+    d.col = (long long)(b / kTile) * rows * kTile + (b % kTile);
+    rays[b] = d;
+    flags[b] = 0;
+    double2* p1 = pd1 + (size_t)b * kSets * CR_MAX_NP;
+    double2* p2 = pd2 + (size_t)b * kSets * CR_MAX_NP;
+    for (int k = 0; k < kSets * CR_MAX_NP; ++k) {
+        p1[k] = make_double2(0.0, 0.0);
+        p2[k] = make_double2(0.0, 0.0);
+    }
+    p2[0] = make_double2(-1.0, 0.0);
+    pd_n[b * kSets + 0] = 1;
+    cr::cd a[CR_MAX_NP], c[CR_MAX_NP];
+    const int ips[3] = {2, 1, 1};
+    const int nss[3] = {r.ns, r.ns, 0};
+    for (int s = 1; s < kSets; ++s) {
+        if (cr::pade_coefficients(r.freq, r.c0, r.np, nss[s - 1], r.dr, ips[s - 1], a, c) != cr::kPadeOk) {
+            atomicOr(status, 1);
+            pd_n[b * kSets + s] = 1;  // keeps the march in bounds; the call reports CR_EPADE
+            continue;
+        }
+        for (int j = 0; j < r.np; ++j) {
+            p1[s * CR_MAX_NP + j] = make_double2(a[j].re, a[j].im);
+            p2[s * CR_MAX_NP + j] = make_double2(c[j].re, c[j].im);
+        }
+        pd_n[b * kSets + s] = r.np;
+    }
+}
+
+// Bit 1 of *status: some ray produced a non-finite field.
+__global__ void static_flags_kernel(const int* flags, int n, int* status) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        if (flags[i]) atomicOr(status, 2);
+}
+
+}  // namespace
+
+extern "C" int cr_march_static(const cr_batch* b, const cr_outputs* out, void* stream_v) {
+    const std::string msg = [&]() -> std::string {
+        if (!out || !out->tll || !out->cpl) return "dev_out with tll and cpl device pointers is required";
+        return std::string();
+    }();
+    if (!msg.empty()) {
+        set_global_error("cr_march_static: %s", msg.c_str());
+        return CR_EINVAL;
+    }
+    const std::string bad = validate(b);
+    if (!bad.empty()) {
+        set_global_error("cr_march_static: %s", bad.c_str());
+        return CR_EINVAL;
+    }
+    if (b->precision != CR_PLAIN_C128) {
+        set_global_error("cr_march_static: only the plain complex128 form is supported");
+        return CR_EINVAL;
+    }
+    if (b->compute_grids && (!out->tlg || !out->cpg)) {
+        set_global_error("cr_march_static: compute_grids needs tlg and cpg device pointers");
+        return CR_EINVAL;
+    }
+    StaticLayout L;
+    static_layout(b, &L);
+    if (L.total > (size_t)CR_STATIC_SCRATCH_BYTES) {
+        set_global_error("cr_march_static: batch needs %zu bytes of scratch, the library holds %u "
+                         "(CR_STATIC_SCRATCH_BYTES); use cr_create/cr_run or a smaller batch",
+                         L.total, (unsigned)CR_STATIC_SCRATCH_BYTES);
+        return CR_EINVAL;
+    }
+    int dev = 0;
+    cudaError_t ce = cudaGetDevice(&dev);
+    if (ce != cudaSuccess) {
+        set_global_error("cr_march_static: %s", cudaGetErrorString(ce));
+        return CR_ECUDA;
+    }
+    void* base_v = nullptr;
+    int rc = static_scratch_ptr(dev, &base_v);
+    if (rc) return rc;
+    unsigned char* base = (unsigned char*)base_v;
+    cudaStream_t st = (cudaStream_t)stream_v;
+    auto h2d = [&](size_t off, const void* src, size_t bytes) {
+        if (ce == cudaSuccess && bytes) ce = cudaMemcpyAsync(base + off, src, bytes, cudaMemcpyHostToDevice, st);
+    };
+    h2d(L.rays_raw, b->rays, (size_t)b->n_rays * sizeof(cr_ray));
+    h2d(L.envs, b->envs, (size_t)b->n_envs * sizeof(cr_env));
+    h2d(L.pool, b->pool, (size_t)b->pool_len * sizeof(double));
+    const int n_slots = L.n_tiles * kTile;
+    if (ce == cudaSuccess) {
+        static_setup_kernel<<<(n_slots + 127) / 128, 128, 0, st>>>(
+            (const cr_ray*)(base + L.rays_raw), b->n_rays, b->compute_grids, L.rows, (RayDev*)(base + L.rays),
+            (int*)(base + L.tile_ray), (double2*)(base + L.pd1), (double2*)(base + L.pd2), (int*)(base + L.pd_n),
+            (int*)(base + L.flags), (int*)(base + L.status), n_slots);
+        ce = cudaGetLastError();
+    }
+    MarchArgs a;
+    a.rays = (const RayDev*)(base + L.rays);
+    a.tile_ray = (const int*)(base + L.tile_ray);
+    a.envs = (const EnvDev*)(base + L.envs);
+    a.pool = (const double*)(base + L.pool);
+    a.pd1 = (const double2*)(base + L.pd1);
+    a.pd2 = (const double2*)(base + L.pd2);
+    a.pd_n = (const int*)(base + L.pd_n);
+    a.f1 = (float*)(base + L.f1);
+    a.f2 = (float*)(base + L.f2);
+    a.f3 = (float*)(base + L.f3);
+    a.ksq = (float2*)(base + L.ksq);
+    a.u = (double2*)(base + L.u);
+    a.W = (double2*)(base + L.W);
+    a.G = (double2*)(base + L.G);
+    a.tll = out->tll;
+    a.cpl = (double2*)out->cpl;
+    a.tlg = b->compute_grids ? out->tlg : nullptr;
+    a.cpg = b->compute_grids ? (double2*)out->cpg : nullptr;
+    a.flags = (int*)(base + L.flags);
+    a.compute_grids = b->compute_grids;
+    if (ce == cudaSuccess) {
+        march_kernel<<<L.n_tiles, kTile, 0, st>>>(a);
+        ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) {
+        static_flags_kernel<<<32, 256, 0, st>>>((const int*)(base + L.flags), b->n_rays, (int*)(base + L.status));
+        ce = cudaGetLastError();
+    }
+    int status = 0;
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(&status, base + L.status, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(st);
+    if (ce != cudaSuccess) {
+        set_global_error("cr_march_static: %s", cudaGetErrorString(ce));
+        return ce == cudaErrorMemoryAllocation ? CR_ENOMEM : CR_ECUDA;
+    }
+    if (status & 1) {
+        set_global_error("cr_march_static: Laguerre method not converging for a Pade set");
+        return CR_EPADE;
+    }
+    if (status & 2) {
+        set_global_error("cr_march_static: a ray produced a non-finite field");
+        return CR_ENAN;
+    }
+    return CR_OK;
+}

@@ -116,3 +116,37 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+
+def march_static(batch: Batch, dev_out, stream=0):
+    """Run ``cr_march_static``: a whole march that allocates nothing.
+
+    For callers that must not allocate device memory when they march (see the
+    cr_march_static comment in include/cupyram_b200.h).  ``dev_out`` maps
+    "tll", "cpl" (and "tlg", "cpg" when the batch computes grids) to device
+    buffers the caller owns - objects with ``data_ptr()`` (e.g. CUDA torch
+    tensors) or raw integer device addresses - laid out like
+    :meth:`Engine.download`'s outputs.  ``stream`` is a raw cudaStream_t
+    handle (0: the default stream).  The scratch holds
+    ``CR_STATIC_SCRATCH_BYTES``; larger batches raise ``ValueError``.
+    """
+    lib = _lib.load()
+    rays = np.ascontiguousarray(batch.rays)
+    envs = np.ascontiguousarray(batch.envs)
+    pool = np.ascontiguousarray(batch.pool, dtype=np.float64)
+    desc = _lib.CrBatch()
+    desc.n_rays, desc.n_envs = len(rays), len(envs)
+    desc.rays, desc.envs, desc.pool = rays.ctypes.data, envs.ctypes.data, pool.ctypes.data
+    desc.pool_len = pool.size
+    desc.precision = _lib.CR_PLAIN_C128
+    desc.compute_grids = 1 if batch.compute_grids else 0
+    desc.line_len, desc.grid_len = batch.line_len, batch.grid_len
+
+    def ptr(name):
+        a = dev_out.get(name)
+        if a is None:
+            return None
+        return int(a) if isinstance(a, int) else int(a.data_ptr())
+
+    o = _lib.CrOutputs(ptr("tll"), ptr("cpl"), ptr("tlg"), ptr("cpg"))
+    _lib.check(lib.cr_march_static(ctypes.byref(desc), ctypes.byref(o), ctypes.c_void_p(stream or None)))

@@ -183,6 +183,53 @@ int cr_global_error(char* buf, size_t len);
 
 void cr_destroy(cr_engine* e);
 
+/*
+ * Size in bytes of the device scratch built into the library for
+ * cr_march_static (a file-scope device array; every GPU that loads the
+ * library holds it until the process exits).
+ */
+#define CR_STATIC_SCRATCH_BYTES (32u * 1024u * 1024u)
+
+/*
+ * cr_march_static - the whole march without allocating anything.
+ *
+ * No counterpart in the reference: CuPyRAM allocates its device arrays with
+ * CuPy for every run.  This entry point is for callers that cannot allocate
+ * device memory at the moment they want a march: a real-time sonar or
+ * tactical-decision loop that forbids allocation after start-up (an
+ * allocation can take unbounded time and may synchronise the device), or a
+ * plug-in running inside a host application whose device memory is owned by
+ * that application's own pool, where an extra cudaMalloc fails or fragments
+ * the pool.  The caller owns the outputs; the per-ray tables, Pade
+ * coefficients (computed on the device), environments and the march
+ * workspace live in the library's CR_STATIC_SCRATCH_BYTES of device scratch.
+ *
+ *   batch    host description, as for cr_create (rays, envs and pool in host
+ *            memory).  Limit: the batch's scratch need (per-ray tables, the
+ *            pool, and 68 bytes per row per ray of march workspace, rows
+ *            counted as the batch's deepest nz + 2 for every ray) must not
+ *            exceed CR_STATIC_SCRATCH_BYTES; otherwise CR_EINVAL with the
+ *            required size in cr_global_error.
+ *   dev_out  DEVICE pointers: tll [line_len] doubles and cpl [line_len]
+ *            complex (interleaved); tlg / cpg [grid_len] when
+ *            batch->compute_grids is set.  Same ragged layout as cr_download.
+ *   stream   cudaStream_t as void* (NULL: the legacy default stream).
+ *
+ * Returns after the march has finished on `stream`.  Calls no cudaMalloc,
+ * cudaFree or other allocating routine; on success it takes no host heap
+ * memory either (a failure stores its message for cr_global_error).
+ * The first call on a device does a one-time set-up with that device
+ * current: it looks up the scratch array's device address
+ * (cudaGetSymbolAddress), and the driver loads the library's kernels and
+ * their fixed local memory.  Make that first call during the caller's own
+ * initialisation, before any stream capture.  Every call shares the one scratch array and
+ * it keeps the last call's contents (everything a march needs is rewritten
+ * or cleared by the call itself), so calls whose work overlaps on the GPU -
+ * from two threads, or on two streams of one device - race and must be
+ * serialised by the caller.  Only the plain complex128 form is supported.
+ */
+int cr_march_static(const cr_batch* batch, const cr_outputs* dev_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

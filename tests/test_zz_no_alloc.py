@@ -1,0 +1,73 @@
+"""cr_march_static - the allocation-free march - against the allocating path.
+
+Some callers cannot allocate device memory when they want a march: a
+real-time loop that forbids allocation after its start-up, or a plug-in whose
+host application owns all device memory through its own pool.  For them the
+library keeps its march scratch in a fixed device array of
+CR_STATIC_SCRATCH_BYTES and cr_march_static writes only into the caller's
+output buffers.  This file is named so that pytest collects it last.
+
+Each check runs the same batch through cr_run (the allocating entry point)
+and through cr_march_static, twice in a row, and compares the TL and
+complex-pressure lines within the engine's parity tolerance (1e-3 dB; the
+two paths differ only in where the Pade coefficients are computed: host or
+device FP64).
+"""
+import numpy as np
+import pytest
+
+from cupyram_b200 import _lib
+from cupyram_b200 import batch as B
+from cupyram_b200.engine import Engine, march_static
+from golden_cases import load_case
+
+pytestmark = pytest.mark.gpu
+
+TOL_DB = 1e-3
+
+
+def _batch(name, grids):
+    args, kw, _ = load_case(name)
+    envs, p, zs, zr, pr = B.prepare(*args, dict(kw))
+    return B.build_batch(envs, p, zs, zr, pr, grids)
+
+
+def _device_outputs(torch, b):
+    out = {"tll": torch.full((max(b.line_len, 1),), float("nan"), dtype=torch.float64, device="cuda"),
+           "cpl": torch.zeros(max(b.line_len, 1), dtype=torch.complex128, device="cuda")}
+    if b.compute_grids:
+        out["tlg"] = torch.full((max(b.grid_len, 1),), float("nan"), dtype=torch.float64, device="cuda")
+        out["cpg"] = torch.zeros(max(b.grid_len, 1), dtype=torch.complex128, device="cuda")
+    return out
+
+
+@pytest.mark.parametrize("name,grids", [("pekeris_small", True), ("ragged_batch", False),
+                                        ("multifreq", True)])
+def test_static_matches_allocating_path(cuda_device, name, grids):
+    import torch
+    b = _batch(name, grids)
+    with Engine(b) as eng:
+        ref = eng.run()
+    n = b.line_len
+    for call in range(2):  # two calls in a row share (and reuse) the scratch
+        out = _device_outputs(torch, b)
+        march_static(b, out, stream=torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        tll = out["tll"].cpu().numpy()[:n]
+        cpl = out["cpl"].cpu().numpy()[:n]
+        assert np.all(np.isfinite(tll)), f"call {call}"
+        assert np.abs(tll - ref["tll"][:n]).max() < TOL_DB, f"call {call}"
+        rel = np.abs(cpl - ref["cpl"][:n]).max() / np.abs(ref["cpl"][:n]).max()
+        assert rel < 1e-6, f"call {call}: {rel}"
+        if grids:
+            g = out["tlg"].cpu().numpy()[:b.grid_len]
+            assert np.percentile(np.abs(g - ref["tlg"][:b.grid_len]), 99.9) < TOL_DB
+
+
+def test_static_rejects_batch_beyond_scratch(cuda_device):
+    import torch
+    from cupyram_b200 import workloads
+    b = workloads.build(*workloads.munk_batch(256, seed=3), compute_grids=False)  # ~100 MB of workspace
+    out = _device_outputs(torch, b)
+    with pytest.raises(ValueError, match="scratch"):
+        march_static(b, out)
