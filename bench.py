@@ -52,6 +52,8 @@ def parse():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-rays", type=int, default=0, help="rays in the CPU sample (0: one per core)")
+    ap.add_argument("--rmax", type=float, default=50000.0,
+                    help="march range (m); shorter values are for profiler captures only")
     return ap.parse_args()
 
 
@@ -65,7 +67,7 @@ def dist_env():
 def workload_config(a, batch):
     return {"workload": f"Munk deep-water batch, {a.rays} rays per GPU, per-ray f U[50,200] Hz, "
                         "zs U[50,1000] m, SSP updates every 5 km (sigma 2 m/s, 1 km corr.), "
-                        "5000 m flat, rmax 50 km, dr 25 m, dz 1 m, np 6, zr 500 m, TL line",
+                        f"5000 m flat, rmax {a.rmax / 1000:g} km, dr 25 m, dz 1 m, np 6, zr 500 m, TL line",
             "rays_per_gpu": int(batch.n_rays), "form": a.form, "seed": a.seed,
             "point_updates_per_gpu": batch.point_updates,
             "nz_range": [int(batch.rays["nz"].min()), int(batch.rays["nz"].max())],
@@ -162,7 +164,7 @@ def run_reference(a):
     if rank != 0:
         return 0
     from cupyram_b200 import workloads
-    batch = workloads.build(*workloads.munk_batch(a.rays, seed=a.seed), compute_grids=False)
+    batch = workloads.build(*workloads.munk_batch(a.rays, seed=a.seed, rmax=a.rmax), compute_grids=False)
     vals = []
     for k in range(a.warmup + a.steps):
         v, dt, n, cores = cpu_sample(batch, a.cpu_rays, a.seed + k, "ref")
@@ -199,7 +201,8 @@ def main():
         pg = dist
     from cupyram_b200 import workloads
     from cupyram_b200.engine import Engine
-    batch = workloads.build(*workloads.munk_batch(a.rays, seed=a.seed + 1000 * rank), compute_grids=False)
+    batch = workloads.build(*workloads.munk_batch(a.rays, seed=a.seed + 1000 * rank, rmax=a.rmax),
+                            compute_grids=False)
     eng = Engine(batch, precision=a.form)
     # pinned host output buffers for the end-to-end path
     out = {"tll": torch.empty(batch.line_len, dtype=torch.float64, pin_memory=True),

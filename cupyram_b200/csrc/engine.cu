@@ -38,6 +38,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -48,445 +49,345 @@
 #include <vector>
 
 #include "../../include/cupyram_b200.h"
+#include "march_common.cuh"
+#include "march_sum.cuh"
 #include "pade.h"
 
 namespace {
 
-constexpr int kTile = 32;  // rays per tile = lanes per warp
+using namespace crk;
 
 // ---------------------------------------------------------------------------
-// device-side descriptors
+// per-lane prefetch ring
+//
+// Every pass streams the rows of one column in order.  Each lane copies its
+// own elements of the next kRing rows into shared memory with cp.async
+// (4/8/16-byte copies; a warp's copies of one row are one coalesced access),
+// so the ~1 us global-memory latency overlaps the serial recurrence of the
+// rows before.  A lane only ever reads its own slots: no warp-wide sync.
 // ---------------------------------------------------------------------------
-struct RayDev {
-    double k0, omega, c0, dz, dr, zmax, lyrw_lambda, attnf, rs, zs, zr;
-    int nz, nr, np, ndr, ndz, nvr, nvz, env;
-    long long line_off, grid_off;
-    long long col;  // element index of (row 0, this lane) in the column arrays
+constexpr int kRing = 32;
+constexpr int kRingFields = 6;
+static_assert((kRing & (kRing - 1)) == 0, "kRing must be a power of two");
+
+// Per slot and lane, six 16-byte fields.  A lane only touches its own
+// column, so the fields are a per-lane union: the on-the-fly passes use
+// {W or u, G, (f1, f2, f3), ksq}; the factorised passes use
+// {W or u, G, S1, S2, S3, AL}.
+struct Ring {
+    double2 q[kRing][kRingFields][kTile];
 };
+constexpr size_t kRingBytes = sizeof(Ring);
 
-struct EnvDev {
-    int n_zss, n_rss, n_zsb, n_rsb, n_bt, pad;
-    long long off;
-};
+enum PassKind { kFirst = 0, kFused = 1, kLast = 2, kEnvOnly = 3 };
 
-// Pade sets per ray: 0 = (1-X)^-2 starter factor, 1 = starter ip=2,
-// 2 = march, 3 = march after the stability range rs.
-constexpr int kSets = 4;
+__device__ __forceinline__ float* ring_f(Ring& R, int slot, int lane) { return (float*)&R.q[slot][2][lane]; }
+__device__ __forceinline__ float2* ring_k(Ring& R, int slot, int lane) { return (float2*)&R.q[slot][3][lane]; }
 
-struct MarchArgs {
-    const RayDev* rays;
-    const int* tile_ray;  // [n_tiles * 32] -> ray index or -1
-    const EnvDev* envs;
-    const double* pool;
-    const double2* pd1;  // [ray][set][CR_MAX_NP]
-    const double2* pd2;
-    const int* pd_n;     // [ray][set]
-    float* f1;
-    float* f2;
-    float* f3;
-    float2* ksq;
-    double2* u;
-    double2* W;
-    double2* G;
-    double* tll;
-    double2* cpl;
-    double* tlg;
-    double2* cpg;
-    int* flags;
-    int compute_grids;
-};
-
-// ---------------------------------------------------------------------------
-// small complex helpers on double2
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ double2 c2(double re, double im) { return make_double2(re, im); }
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-    return c2(fma(a.x, b.x, -a.y * b.y), fma(a.x, b.y, a.y * b.x));
-}
-__device__ __forceinline__ double2 cfms(double2 acc, double2 a, double2 b) {  // acc - a*b
-    return c2(acc.x - fma(a.x, b.x, -a.y * b.y), acc.y - fma(a.x, b.y, a.y * b.x));
-}
-__device__ __forceinline__ double2 crcp(double2 b) {
-    const double inv = 1.0 / fma(b.x, b.x, b.y * b.y);
-    return c2(b.x * inv, -b.y * inv);
-}
-// a + p * d  with real a
-__device__ __forceinline__ double2 caxpd(double a, double2 p, double2 d) {
-    return c2(a + fma(p.x, d.x, -p.y * d.y), fma(p.x, d.y, p.y * d.x));
-}
-
-// ---------------------------------------------------------------------------
-// profile interpolation (profl)
-// ---------------------------------------------------------------------------
-struct EnvPtrs {
-    const double *z_ss, *rp_ss, *cw, *z_sb, *rp_sb, *cb, *rhob, *attn, *rb, *zb;
-    int n_zss, n_rss, n_zsb, n_rsb, n_bt;
-};
-
-__device__ EnvPtrs env_ptrs(const EnvDev& e, const double* pool) {
-    EnvPtrs p;
-    const double* q = pool + e.off;
-    p.n_zss = e.n_zss;
-    p.n_rss = e.n_rss;
-    p.n_zsb = e.n_zsb;
-    p.n_rsb = e.n_rsb;
-    p.n_bt = e.n_bt;
-    p.z_ss = q; q += p.n_zss;
-    p.rp_ss = q; q += p.n_rss;
-    p.cw = q; q += (long long)p.n_rss * p.n_zss;
-    p.z_sb = q; q += p.n_zsb;
-    p.rp_sb = q; q += p.n_rsb;
-    p.cb = q; q += (long long)p.n_rsb * p.n_zsb;
-    p.rhob = q; q += (long long)p.n_rsb * p.n_zsb;
-    p.attn = q; q += (long long)p.n_rsb * p.n_zsb;
-    p.rb = q; q += p.n_bt;
-    p.zb = q;
-    return p;
-}
-
-// index idx with arr[idx] <= v < arr[idx+1] (profl.py:8-35 semantics)
-__device__ __forceinline__ int seg_search(double v, const double* arr, int n) {
-    if (n <= 1 || v <= arr[0]) return 0;
-    if (v >= arr[n - 1]) return n - 2;
-    int lo = 0, hi = n - 1;
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (arr[mid] <= v) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-
-__device__ __forceinline__ double lerp_seg(double x, double x0, double x1, double y0, double y1) {
-    if (x1 == x0) return y0;
-    return y0 + (y1 - y0) * ((x - x0) / (x1 - x0));
-}
-
-struct RowProps {
-    float cw, cb, rhob, attn;
-};
-
-// Interpolated water / seabed properties at depth z for the active profiles,
-// rounded to float32 as the reference stores them.
-__device__ RowProps row_props(const EnvPtrs& e, int ss, int sb, double z, double lyrw_lambda,
-                              double attnf) {
-    RowProps o;
-    const double* cwp = e.cw + (long long)ss * e.n_zss;
-    const int n1 = e.n_zss;
-    double v;
-    if (z <= e.z_ss[0]) v = cwp[0];
-    else if (z >= e.z_ss[n1 - 1]) v = cwp[n1 - 1];
-    else {
-        const int k = seg_search(z, e.z_ss, n1);
-        v = lerp_seg(z, e.z_ss[k], e.z_ss[k + 1], cwp[k], cwp[k + 1]);
-    }
-    o.cw = (float)v;
-    const int n2 = e.n_zsb;
-    const long long so = (long long)sb * n2;
-    const double* cbp = e.cb + so;
-    const double* rhp = e.rhob + so;
-    const double* atp = e.attn + so;
-    const double z0 = e.z_sb[0], zl = e.z_sb[n2 - 1];
-    const int k = seg_search(z, e.z_sb, n2);
-    if (z <= z0) {
-        o.cb = (float)cbp[0];
-        o.rhob = (float)rhp[0];
-    } else if (z >= zl) {
-        o.cb = (float)cbp[n2 - 1];
-        o.rhob = (float)rhp[n2 - 1];
-    } else {
-        o.cb = (float)lerp_seg(z, e.z_sb[k], e.z_sb[k + 1], cbp[k], cbp[k + 1]);
-        o.rhob = (float)lerp_seg(z, e.z_sb[k], e.z_sb[k + 1], rhp[k], rhp[k + 1]);
-    }
-    // attenuation with the absorbing layer: profile, then constant over the
-    // first 75 % of the layer, then a linear ramp to attnf (profl.py:121-140)
-    const double alast = atp[n2 - 1];
-    const double zl1 = zl + 0.75 * lyrw_lambda, zl2 = zl + lyrw_lambda;
-    if (z <= zl) {
-        if (z <= z0) v = atp[0];
-        else v = lerp_seg(z, e.z_sb[k], e.z_sb[k + 1], atp[k], atp[k + 1]);
-    } else if (z <= zl1) {
-        v = alast;
-    } else if (z <= zl2) {
-        v = lerp_seg(z, zl1, zl2, alast, attnf);
-    } else {
-        v = attnf;
-    }
-    o.attn = (float)v;
-    return o;
-}
-
-// Write the layer-selected coefficients of rows [lo, hi] (matrc.py:16-107
-// with iz == jz, preceded by the alpw / alpb / ksqw / ksqb maths of
-// cupyram.py:782-803).
-__device__ void assemble_rows(const RayDev& ry, const EnvPtrs& e, int ss, int sb, int iz, int lo,
-                              int hi, float* f1, float* f2, float* f3, float2* ksq) {
-    const double step = ry.zmax / (double)(ry.nz + 1);
-    const double eta = 1.0 / (40.0 * M_PI * 0.43429448190325176);  // 1/(40 pi log10 e)
-    const double k02 = ry.k0 * ry.k0;
-    for (int i = lo; i <= hi; ++i) {
-        const double z = (i == ry.nz + 1) ? ry.zmax : (double)i * step;
-        const RowProps p = row_props(e, ss, sb, z, ry.lyrw_lambda, ry.attnf);
-        const long long o = ry.col + (long long)i * kTile;
-        if (i <= iz) {
-            const double alpw = sqrt((double)p.cw / ry.c0);
-            const double ow = ry.omega / (double)p.cw;
-            f1[o] = (float)(1.0 / alpw);
-            f2[o] = 1.0f;
-            f3[o] = (float)alpw;
-            ksq[o] = make_float2((float)(ow * ow - k02), 0.0f);
-        } else {
-            const double alpb = sqrt((double)(p.rhob * p.cb) / ry.c0);
-            const double ob = ry.omega / (double)p.cb;
-            const double ti = ob * eta * (double)p.attn;  // term = ob + i*ti
-            f1[o] = (float)((double)p.rhob / alpb);
-            f2[o] = (float)(1.0 / (double)p.rhob);
-            f3[o] = (float)alpb;
-            ksq[o] = make_float2((float)(ob * ob - ti * ti - k02), (float)(2.0 * ob * ti));
+// Issue the copies of stream row r into ring slot `slot` (one commit group,
+// possibly empty when r is outside 0..nz+1).
+template <int KIND>
+__device__ __forceinline__ void ring_issue(Ring& R, const Col& c, int slot, int r, int nz, int lane) {
+    if (r >= 0 && r <= nz + 1) {
+        const long long o = (long long)r * kTile;
+        if (KIND == kFirst) cp16(&R.q[slot][0][lane], c.u + o);
+        else if (KIND != kEnvOnly) {
+            cp16(&R.q[slot][0][lane], c.W + o);
+            cp16(&R.q[slot][1][lane], c.G + o);
+        }
+        if (KIND != kLast) {
+            float* f = ring_f(R, slot, lane);
+            cp4(f + 0, c.f1 + o);
+            cp4(f + 1, c.f2 + o);
+            cp4(f + 2, c.f3 + o);
+            cp8(ring_k(R, slot, lane), c.ksq + o);
         }
     }
+    cp_commit();
 }
 
-// ---------------------------------------------------------------------------
-// Galerkin row: D_i = (d1, d2, d3) from the 3-row window of f1..f3, ksq
-// ---------------------------------------------------------------------------
-struct Win {
-    float f1c, f2m, f2c, f2p, f3m, f3c, f3p;
-    float2 km, kc, kp;
-};
-
-struct Drow {
-    double2 d1, d2, d3;
-};
-
-__device__ __forceinline__ Drow galerkin(const Win& w, double cfact) {
-    const double f1 = w.f1c;
-    const double c1 = cfact * f1 * ((double)w.f2m + (double)w.f2c) * (double)w.f3m;
-    const double c2v = -cfact * f1 * ((double)w.f2m + 2.0 * (double)w.f2c + (double)w.f2p) * (double)w.f3c;
-    const double c3 = cfact * f1 * ((double)w.f2c + (double)w.f2p) * (double)w.f3p;
-    const double df = 1.0 / 12.0;
-    Drow d;
-    d.d1 = c2(c1 + df * ((double)w.km.x + (double)w.kc.x), df * ((double)w.km.y + (double)w.kc.y));
-    d.d2 = c2(c2v + df * ((double)w.km.x + 6.0 * (double)w.kc.x + (double)w.kp.x),
-              df * ((double)w.km.y + 6.0 * (double)w.kc.y + (double)w.kp.y));
-    d.d3 = c2(c3 + df * ((double)w.kc.x + (double)w.kp.x), df * ((double)w.kc.y + (double)w.kp.y));
-    return d;
-}
-
-struct Col {
-    const float* f1;
-    const float* f2;
-    const float* f3;
-    const float2* ksq;
-    double2* u;
-    double2* W;
-    double2* G;
-};
-
-struct StepCtx {
-    Col c;
-    int nz;
-    double cfact, a1, a2;
-    double2 u0;  // field value held at the surface row (non-zero only for zs < dz)
-};
-
-// ---------------------------------------------------------------------------
-// the passes of one range step
-// ---------------------------------------------------------------------------
-// Pass 0: eliminate term 0 downwards reading the step's input field.
-__device__ void pass_first(const StepCtx& s, double2 p1, double2 p2) {
+// One pass over the column.
+//   kFirst, DOWN : eliminate term (p1, p2) downwards from the stored field u.
+//   kFused, DOWN : back-substitute the UP-eliminated term, eliminate (p1, p2) DOWN.
+//   kFused, UP   : back-substitute the DOWN-eliminated term, eliminate (p1, p2) UP.
+//   kLast        : back-substitute the last term (eliminated opposite to DOWN)
+//                  and store the field.
+// Stream row r carries W_r, G_r (or u_r) and f1..f3, ksq of row r; the
+// elimination runs one row behind the stream so that its 3-row windows of
+// field and coefficients are complete.
+template <int KIND, bool DOWN>
+__device__ void run_pass(const StepCtx& s, Ring& R, double2 p1, double2 p2) {
     const Col& c = s.c;
     const int nz = s.nz;
-    Win w;
-    w.f2m = c.f2[0];
-    w.f3m = c.f3[0];
-    w.km = c.ksq[0];
-    w.f1c = c.f1[kTile];
-    w.f2c = c.f2[kTile];
-    w.f3c = c.f3[kTile];
-    w.kc = c.ksq[kTile];
-    double2 xm = s.u0, xc = c.u[kTile];
+    const int lane = threadIdx.x;
+    const int nrows = nz + 2;
+    __threadfence_block();  // order this lane's earlier stores before its cp.async reads
+#pragma unroll 1
+    for (int k = 0; k < kRing; ++k) ring_issue<KIND>(R, c, k, DOWN ? k : nz + 1 - k, nz, lane);
+
+    EnvRow em{}, ec{}, ep{};
+    double2 x0 = c2(0.0, 0.0), x1 = c2(0.0, 0.0), x2 = c2(0.0, 0.0);  // field window, oldest first
     double2 wp = c2(0.0, 0.0), gp = c2(0.0, 0.0);
-    for (int i = 1; i <= nz; ++i) {
-        const long long o = (long long)(i + 1) * kTile;
-        w.f2p = c.f2[o];
-        w.f3p = c.f3[o];
-        w.kp = c.ksq[o];
-        const double2 xp = (i < nz) ? c.u[o] : c2(0.0, 0.0);
-        const float f1n = c.f1[o];
-        const Drow d = galerkin(w, s.cfact);
+    const double2 zero = c2(0.0, 0.0);
+#pragma unroll 1
+    for (int k = 0; k < nrows; ++k) {
+        const int r = DOWN ? k : nz + 1 - k;
+        const int slot = k & (kRing - 1);
+        cp_wait<kRing - 1>();
+        double2 av = zero, bv = zero;
+        EnvRow er{};
+        av = R.q[slot][0][lane];
+        if (KIND != kFirst) bv = R.q[slot][1][lane];
+        if (KIND != kLast) {
+            const float* f = ring_f(R, slot, lane);
+            er.f1 = f[0];
+            er.f2 = f[1];
+            er.f3 = f[2];
+            er.k = *ring_k(R, slot, lane);
+        }
+        ring_issue<KIND>(R, c, slot, DOWN ? k + kRing : nz + 1 - k - kRing, nz, lane);
+
+        // field value x_r of this stream row
+        double2 xr;
+        if (KIND == kFirst) {
+            xr = (r == 0) ? s.u0 : (r == nz + 1 ? zero : av);
+        } else if (DOWN) {  // previous term was eliminated UP: x_r = g_r - w_r x_{r-1}
+            xr = (r == 0) ? s.u0 : (r == nz + 1 ? zero : (r == 1 ? bv : cfms(bv, av, x2)));
+        } else {  // previous term eliminated DOWN: x_r = g_r - w_r x_{r+1}
+            xr = (r == nz + 1) ? zero : (r == 0 ? s.u0 : (r == nz ? bv : cfms(bv, av, x2)));
+        }
+        if (KIND == kLast) {
+            if (r >= 1 && r <= nz) c.u[(long long)r * kTile] = xr;
+            x2 = xr;
+            continue;
+        }
+        x0 = x1;
+        x1 = x2;
+        x2 = xr;
+        if (DOWN) {
+            em = ec;
+            ec = ep;
+            ep = er;
+        } else {
+            ep = ec;
+            ec = em;
+            em = er;
+        }
+        if (k < 2) continue;
+        // eliminate row m: DOWN m = r-1 with (x_{m-1}, x_m, x_{m+1}) = (x0, x1, x2);
+        //                  UP   m = r+1 with (x_{m-1}, x_m, x_{m+1}) = (x2, x1, x0)
+        const int m = DOWN ? r - 1 : r + 1;
+        if (m < 1 || m > nz) continue;
+        const Drow d = galerkin3(em, ec, ep, s.cfact);
         const double2 r1 = caxpd(s.a1, p2, d.d1), r2 = caxpd(s.a2, p2, d.d2), r3 = caxpd(s.a1, p2, d.d3);
         const double2 q1 = caxpd(s.a1, p1, d.d1), q2 = caxpd(s.a2, p1, d.d2), q3 = caxpd(s.a1, p1, d.d3);
-        double2 rhs = cmul(q1, xm);
-        rhs = c2(rhs.x + (q2.x * xc.x - q2.y * xc.y) + (q3.x * xp.x - q3.y * xp.y),
-                 rhs.y + (q2.x * xc.y + q2.y * xc.x) + (q3.x * xp.y + q3.y * xp.x));
-        const double2 inv = crcp(cfms(r2, r1, wp));
-        wp = cmul(r3, inv);
-        gp = cmul(cfms(rhs, r1, gp), inv);
-        const long long oi = (long long)i * kTile;
-        c.W[oi] = wp;
-        c.G[oi] = gp;
-        xm = xc;
-        xc = xp;
-        w.f2m = w.f2c; w.f3m = w.f3c; w.km = w.kc;
-        w.f1c = f1n; w.f2c = w.f2p; w.f3c = w.f3p; w.kc = w.kp;
+        const double2 xlo = DOWN ? x0 : x2, xhi = DOWN ? x2 : x0;
+        double2 rhs = cmul(q1, xlo);
+        rhs = c2(rhs.x + (q2.x * x1.x - q2.y * x1.y) + (q3.x * xhi.x - q3.y * xhi.y),
+                 rhs.y + (q2.x * x1.y + q2.y * x1.x) + (q3.x * xhi.y + q3.y * xhi.x));
+        // DOWN: couple to the row above (r1), continue with r3; UP: the reverse
+        const double2 cin = DOWN ? r1 : r3, cout = DOWN ? r3 : r1;
+        const double2 inv = crcp(cfms(r2, cin, wp));
+        wp = cmul(cout, inv);
+        gp = cmul(cfms(rhs, cin, gp), inv);
+        const long long om = (long long)m * kTile;
+        c.W[om] = wp;
+        c.G[om] = gp;
     }
+    cp_wait<0>();
 }
 
-// Fused pass going DOWN: back-substitute a term that was eliminated UP
-// (x_i = g_i - w_i x_{i-1}) and eliminate the next term DOWN one row behind.
-__device__ void pass_fused_down(const StepCtx& s, double2 p1, double2 p2) {
-    const Col& c = s.c;
-    const int nz = s.nz;
-    Win w;
-    w.f2m = c.f2[0];
-    w.f3m = c.f3[0];
-    w.km = c.ksq[0];
-    w.f1c = c.f1[kTile];
-    w.f2c = c.f2[kTile];
-    w.f3c = c.f3[kTile];
-    w.kc = c.ksq[kTile];
-    double2 xmm = s.u0;  // x_{i-2}
-    double2 xm = s.u0;   // x_{i-1}; at i = 1 the back-substitution starts from x_0
-    double2 wp = c2(0.0, 0.0), gp = c2(0.0, 0.0);
-    // back-substitution of the previous term: x_1 = g'_1, x_i = g'_i - w'_i x_{i-1}
-    for (int i = 1; i <= nz + 1; ++i) {
-        double2 xc;
-        if (i <= nz) {
-            const long long oi = (long long)i * kTile;
-            const double2 wi = c.W[oi], gi = c.G[oi];
-            xc = (i == 1) ? gi : cfms(gi, wi, xm);
-        } else {
-            xc = c2(0.0, 0.0);
-        }
-        if (i >= 2) {
-            // eliminate row m = i-1 (needs x_{m-1} = xmm, x_m = xm, x_{m+1} = xc)
-            const int m = i - 1;
-            const long long o = (long long)(m + 1) * kTile;
-            w.f2p = c.f2[o];
-            w.f3p = c.f3[o];
-            w.kp = c.ksq[o];
-            const float f1n = (m + 1 <= nz + 1) ? c.f1[o] : 0.0f;
-            const Drow d = galerkin(w, s.cfact);
-            const double2 r1 = caxpd(s.a1, p2, d.d1), r2 = caxpd(s.a2, p2, d.d2), r3 = caxpd(s.a1, p2, d.d3);
-            const double2 q1 = caxpd(s.a1, p1, d.d1), q2 = caxpd(s.a2, p1, d.d2), q3 = caxpd(s.a1, p1, d.d3);
-            double2 rhs = cmul(q1, xmm);
-            rhs = c2(rhs.x + (q2.x * xm.x - q2.y * xm.y) + (q3.x * xc.x - q3.y * xc.y),
-                     rhs.y + (q2.x * xm.y + q2.y * xm.x) + (q3.x * xc.y + q3.y * xc.x));
-            const double2 inv = crcp(cfms(r2, r1, wp));
-            wp = cmul(r3, inv);
-            gp = cmul(cfms(rhs, r1, gp), inv);
-            const long long om = (long long)m * kTile;
-            c.W[om] = wp;
-            c.G[om] = gp;
-            w.f2m = w.f2c; w.f3m = w.f3c; w.km = w.kc;
-            w.f1c = f1n; w.f2c = w.f2p; w.f3c = w.f3p; w.kc = w.kp;
-        }
-        xmm = xm;
-        xm = xc;
-    }
-}
-
-// Fused pass going UP: back-substitute a term eliminated DOWN
-// (x_i = g_i - w_i x_{i+1}) and eliminate the next term UP one row behind.
-__device__ void pass_fused_up(const StepCtx& s, double2 p1, double2 p2) {
-    const Col& c = s.c;
-    const int nz = s.nz;
-    // Window rows (m-1, m, m+1) for m = i+1 once row i is loaded.  Each
-    // iteration rotates p <- c <- m <- (row i); the "m" slot starts with row
-    // nz+1 so that the first elimination (m = nz) sees rows nz-1, nz, nz+1.
-    Win w;
-    {
-        const long long o = (long long)(nz + 1) * kTile;
-        w.f2m = c.f2[o];
-        w.f3m = c.f3[o];
-        w.km = c.ksq[o];
-        w.f1c = 0.0f;
-        w.f2c = 0.0f; w.f3c = 0.0f; w.kc = make_float2(0.f, 0.f);
-        w.f2p = 0.0f; w.f3p = 0.0f; w.kp = make_float2(0.f, 0.f);
-    }
-    double2 xpp = c2(0.0, 0.0);  // x_{i+2}
-    double2 xp = c2(0.0, 0.0);   // x_{i+1}
-    double2 wp = c2(0.0, 0.0), gp = c2(0.0, 0.0);
-    for (int i = nz; i >= 0; --i) {
-        double2 xc;
-        if (i >= 1) {
-            const long long oi = (long long)i * kTile;
-            const double2 wi = c.W[oi], gi = c.G[oi];
-            xc = (i == nz) ? gi : cfms(gi, wi, xp);
-        } else {
-            xc = s.u0;
-        }
-        // slide the window down one row: load row i as the new "m-1"
-        const long long o = (long long)i * kTile;
-        const float f1i = c.f1[o];
-        const float f2i = c.f2[o];
-        const float f3i = c.f3[o];
-        const float2 ki = c.ksq[o];
-        w.f2p = w.f2c; w.f3p = w.f3c; w.kp = w.kc;
-        w.f2c = w.f2m; w.f3c = w.f3m; w.kc = w.km;  // (previous "m-1" becomes "m")
-        w.f2m = f2i; w.f3m = f3i; w.km = ki;
-        const float f1m_next = f1i;
-        if (i <= nz - 1) {
-            // eliminate row m = i+1 (needs x_i = xc, x_{m} = xp, x_{m+1} = xpp)
-            const int m = i + 1;
-            const Drow d = galerkin(w, s.cfact);
-            const double2 r1 = caxpd(s.a1, p2, d.d1), r2 = caxpd(s.a2, p2, d.d2), r3 = caxpd(s.a1, p2, d.d3);
-            const double2 q1 = caxpd(s.a1, p1, d.d1), q2 = caxpd(s.a2, p1, d.d2), q3 = caxpd(s.a1, p1, d.d3);
-            double2 rhs = cmul(q1, xc);
-            rhs = c2(rhs.x + (q2.x * xp.x - q2.y * xp.y) + (q3.x * xpp.x - q3.y * xpp.y),
-                     rhs.y + (q2.x * xp.y + q2.y * xp.x) + (q3.x * xpp.y + q3.y * xpp.x));
-            const double2 inv = crcp(cfms(r2, r3, wp));
-            wp = cmul(r1, inv);
-            gp = cmul(cfms(rhs, r3, gp), inv);
-            const long long om = (long long)m * kTile;
-            c.W[om] = wp;
-            c.G[om] = gp;
-        }
-        w.f1c = f1m_next;  // f1 of the row that becomes "m" at the next iteration
-        xpp = xp;
-        xp = xc;
-    }
-}
-
-// Last pass: back-substitute the last term and store the field.
-__device__ void pass_last(const StepCtx& s, bool last_elim_down) {
-    const Col& c = s.c;
-    const int nz = s.nz;
-    if (last_elim_down) {
-        double2 xp = c2(0.0, 0.0);
-        for (int i = nz; i >= 1; --i) {
-            const long long oi = (long long)i * kTile;
-            const double2 gi = c.G[oi];
-            const double2 xc = (i == nz) ? gi : cfms(gi, c.W[oi], xp);
-            c.u[oi] = xc;
-            xp = xc;
-        }
-    } else {
-        double2 xm = s.u0;
-        for (int i = 1; i <= nz; ++i) {
-            const long long oi = (long long)i * kTile;
-            const double2 gi = c.G[oi];
-            const double2 xc = (i == 1) ? gi : cfms(gi, c.W[oi], xm);
-            c.u[oi] = xc;
-            xm = xc;
-        }
-    }
-}
-
-// Pass 0 with the elimination running UP is never needed: term 0 always
-// eliminates DOWN.  The eliminations go DOWN for even terms, UP for odd ones.
-__device__ void pe_step(const StepCtx& s, const double2* p1, const double2* p2, int n) {
-    pass_first(s, p1[0], p2[0]);
+// Term 0 eliminates DOWN from the stored field; term t eliminates DOWN when t
+// is even and UP when t is odd, fused with the back-substitution of term t-1.
+__device__ void pe_step(const StepCtx& s, Ring& R, const double2* p1, const double2* p2, int n) {
+    run_pass<kFirst, true>(s, R, p1[0], p2[0]);
     for (int t = 1; t < n; ++t) {
-        if (t & 1) pass_fused_up(s, p1[t], p2[t]);
-        else pass_fused_down(s, p1[t], p2[t]);
+        if (t & 1) run_pass<kFused, false>(s, R, p1[t], p2[t]);
+        else run_pass<kFused, true>(s, R, p1[t], p2[t]);
     }
-    pass_last(s, ((n - 1) & 1) == 0);
+    // last term eliminated DOWN (n-1 even) -> back-substitute UP, and vice versa
+    if (((n - 1) & 1) == 0) run_pass<kLast, false>(s, R, c2(0, 0), c2(0, 0));
+    else run_pass<kLast, true>(s, R, c2(0, 0), c2(0, 0));
 }
 
-__device__ __forceinline__ double tl_db(double amp, double r) {
-    return -20.0 * log10(amp + 1e-20) + 10.0 * log10(r + 1e-20);
+// ---------------------------------------------------------------------------
+// factorised march: the operator of a term is fixed until the environment
+// (profiles, bathymetry index) or the Pade set changes, so its Thomas
+// factorisation - the expensive, strictly serial part with a division per
+// row - is computed once per change and every range step only runs
+//     g_m = S1 x_{m-1} + S2 x_m + S3 x_{m+1} + AL g_{m-/+1}     (elimination)
+//     x_m = g_m - WF x_{m+/-1}                                  (back-substitution)
+// with S_k = s_k / den_m, AL = -(coupling) / den_m, WF = w_m.
+// ---------------------------------------------------------------------------
+struct Fac {
+    double2 *S1, *S2, *S3, *AL, *WF;  // already offset to (term, row 0, lane)
+};
+
+__device__ __forceinline__ Fac fac_term(const MarchArgs& a, const RayDev& ry, int t) {
+    const long long o = ry.ccol + (long long)t * ry.crows * kTile;
+    return Fac{a.S1 + o, a.S2 + o, a.S3 + o, a.AL + o, a.WF + o};
+}
+
+// Factorise one term (pd1 = p1, pd2 = p2) eliminating DOWN or UP.
+template <bool DOWN>
+__device__ void factor_pass(const StepCtx& s, Ring& R, double2 p1, double2 p2, const Fac& f) {
+    const Col& c = s.c;
+    const int nz = s.nz;
+    const int lane = threadIdx.x;
+    const int nrows = nz + 2;
+    __threadfence_block();
+#pragma unroll 1
+    for (int k = 0; k < kRing; ++k) ring_issue<kEnvOnly>(R, c, k, DOWN ? k : nz + 1 - k, nz, lane);
+    EnvRow em{}, ec{}, ep{};
+    double2 wp = c2(0.0, 0.0);
+#pragma unroll 1
+    for (int k = 0; k < nrows; ++k) {
+        const int r = DOWN ? k : nz + 1 - k;
+        const int slot = k & (kRing - 1);
+        cp_wait<kRing - 1>();
+        EnvRow er;
+        {
+            const float* fl = ring_f(R, slot, lane);
+            er.f1 = fl[0];
+            er.f2 = fl[1];
+            er.f3 = fl[2];
+            er.k = *ring_k(R, slot, lane);
+        }
+        ring_issue<kEnvOnly>(R, c, slot, DOWN ? k + kRing : nz + 1 - k - kRing, nz, lane);
+        if (DOWN) {
+            em = ec;
+            ec = ep;
+            ep = er;
+        } else {
+            ep = ec;
+            ec = em;
+            em = er;
+        }
+        if (k < 2) continue;
+        const int m = DOWN ? r - 1 : r + 1;
+        if (m < 1 || m > nz) continue;
+        const Drow d = galerkin3(em, ec, ep, s.cfact);
+        const double2 r1 = caxpd(s.a1, p2, d.d1), r2 = caxpd(s.a2, p2, d.d2), r3 = caxpd(s.a1, p2, d.d3);
+        const double2 q1 = caxpd(s.a1, p1, d.d1), q2 = caxpd(s.a2, p1, d.d2), q3 = caxpd(s.a1, p1, d.d3);
+        const double2 cin = DOWN ? r1 : r3, cout = DOWN ? r3 : r1;
+        const double2 inv = crcp(cfms(r2, cin, wp));
+        wp = cmul(cout, inv);
+        const long long om = (long long)m * kTile;
+        f.S1[om] = cmul(q1, inv);
+        f.S2[om] = cmul(q2, inv);
+        f.S3[om] = cmul(q3, inv);
+        const double2 ci = cmul(cin, inv);
+        f.AL[om] = c2(-ci.x, -ci.y);
+        f.WF[om] = wp;
+    }
+    cp_wait<0>();
+}
+
+// Stream row r of a factorised pass: field or W of the previous term, G, and
+// the elimination factors of row m = r -/+ 1 of the current term.
+template <int KIND, bool DOWN>
+__device__ __forceinline__ void ring_issue_fac(Ring& R, const Col& c, int slot, int r, int nz, int lane,
+                                               const double2* Wprev, const Fac& f) {
+    if (r >= 0 && r <= nz + 1) {
+        const long long o = (long long)r * kTile;
+        if (KIND == kFirst) cp16(&R.q[slot][0][lane], c.u + o);
+        else {
+            cp16(&R.q[slot][0][lane], Wprev + o);
+            cp16(&R.q[slot][1][lane], c.G + o);
+        }
+        const int m = DOWN ? r - 1 : r + 1;
+        if (KIND != kLast && m >= 1 && m <= nz) {
+            const long long om = (long long)m * kTile;
+            cp16(&R.q[slot][2][lane], f.S1 + om);
+            cp16(&R.q[slot][3][lane], f.S2 + om);
+            cp16(&R.q[slot][4][lane], f.S3 + om);
+            cp16(&R.q[slot][5][lane], f.AL + om);
+        }
+    }
+    cp_commit();
+}
+
+// One factorised pass (same stream order and one-row lag as run_pass).
+template <int KIND, bool DOWN>
+__device__ void run_pass_fac(const StepCtx& s, Ring& R, const double2* Wprev, const Fac& f) {
+    const Col& c = s.c;
+    const int nz = s.nz;
+    const int lane = threadIdx.x;
+    const int nrows = nz + 2;
+    __threadfence_block();
+#pragma unroll 1
+    for (int k = 0; k < kRing; ++k)
+        ring_issue_fac<KIND, DOWN>(R, c, k, DOWN ? k : nz + 1 - k, nz, lane, Wprev, f);
+    double2 x0 = c2(0.0, 0.0), x1 = c2(0.0, 0.0), x2 = c2(0.0, 0.0);
+    double2 gp = c2(0.0, 0.0);
+    const double2 zero = c2(0.0, 0.0);
+#pragma unroll 1
+    for (int k = 0; k < nrows; ++k) {
+        const int r = DOWN ? k : nz + 1 - k;
+        const int slot = k & (kRing - 1);
+        cp_wait<kRing - 1>();
+        const double2 av = R.q[slot][0][lane];
+        double2 bv = zero, s1 = zero, s2 = zero, s3 = zero, al = zero;
+        if (KIND != kFirst) bv = R.q[slot][1][lane];
+        if (KIND != kLast) {
+            s1 = R.q[slot][2][lane];
+            s2 = R.q[slot][3][lane];
+            s3 = R.q[slot][4][lane];
+            al = R.q[slot][5][lane];
+        }
+        ring_issue_fac<KIND, DOWN>(R, c, slot, DOWN ? k + kRing : nz + 1 - k - kRing, nz, lane, Wprev, f);
+        // x_r = g_r - w_r x_prev as two dependent FMAs per component
+        const double2 xb = c2(fma(-av.x, x2.x, fma(av.y, x2.y, bv.x)), fma(-av.x, x2.y, fma(-av.y, x2.x, bv.y)));
+        double2 xr;
+        if (KIND == kFirst) {
+            xr = (r == 0) ? s.u0 : (r == nz + 1 ? zero : av);
+        } else if (DOWN) {
+            xr = (r == 0) ? s.u0 : (r == nz + 1 ? zero : (r == 1 ? bv : xb));
+        } else {
+            xr = (r == nz + 1) ? zero : (r == 0 ? s.u0 : (r == nz ? bv : xb));
+        }
+        if (KIND == kLast) {
+            if (r >= 1 && r <= nz) c.u[(long long)r * kTile] = xr;
+            x2 = xr;
+            continue;
+        }
+        x0 = x1;
+        x1 = x2;
+        x2 = xr;
+        if (k < 2) continue;
+        const int m = DOWN ? r - 1 : r + 1;
+        if (m < 1 || m > nz) continue;
+        const double2 xlo = DOWN ? x0 : x2, xhi = DOWN ? x2 : x0;
+        // the two older field values first, then the new one, then the recurrence
+        double2 t = c2(fma(s1.x, xlo.x, fma(-s1.y, xlo.y, fma(s2.x, x1.x, -s2.y * x1.y))),
+                       fma(s1.x, xlo.y, fma(s1.y, xlo.x, fma(s2.x, x1.y, s2.y * x1.x))));
+        t = c2(fma(s3.x, xhi.x, fma(-s3.y, xhi.y, t.x)), fma(s3.x, xhi.y, fma(s3.y, xhi.x, t.y)));
+        const double2 g = c2(fma(al.x, gp.x, fma(-al.y, gp.y, t.x)), fma(al.x, gp.y, fma(al.y, gp.x, t.y)));
+        gp = g;
+        c.G[(long long)m * kTile] = g;
+    }
+    cp_wait<0>();
+}
+
+__device__ void factor_set(const StepCtx& s, Ring& R, const MarchArgs& a, const RayDev& ry,
+                           const double2* p1, const double2* p2, int n) {
+    for (int t = 0; t < n; ++t) {
+        const Fac f = fac_term(a, ry, t);
+        if (t & 1) factor_pass<false>(s, R, p1[t], p2[t], f);
+        else factor_pass<true>(s, R, p1[t], p2[t], f);
+    }
+}
+
+__device__ void pe_step_fac(const StepCtx& s, Ring& R, const MarchArgs& a, const RayDev& ry, int n) {
+    run_pass_fac<kFirst, true>(s, R, nullptr, fac_term(a, ry, 0));
+    for (int t = 1; t < n; ++t) {
+        const double2* wprev = fac_term(a, ry, t - 1).WF;
+        if (t & 1) run_pass_fac<kFused, false>(s, R, wprev, fac_term(a, ry, t));
+        else run_pass_fac<kFused, true>(s, R, wprev, fac_term(a, ry, t));
+    }
+    const Fac last = fac_term(a, ry, n - 1);
+    if (((n - 1) & 1) == 0) run_pass_fac<kLast, false>(s, R, last.WF, last);
+    else run_pass_fac<kLast, true>(s, R, last.WF, last);
 }
 
 // Receiver line and TL grid after a step (outpt.py:11-57).  The CP grid is
@@ -524,6 +425,8 @@ __device__ void write_outputs(const MarchArgs& a, const RayDev& ry, const Col& c
 // the march kernel: one lane = one ray, all steps
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kTile) march_kernel(MarchArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    Ring& ring = *reinterpret_cast<Ring*>(smem_raw);
     const int rid = a.tile_ray[blockIdx.x * kTile + threadIdx.x];
     if (rid < 0) return;
     const RayDev ry = a.rays[rid];
@@ -574,9 +477,9 @@ __global__ void __launch_bounds__(kTile) march_kernel(MarchArgs a) {
     const double2* pd1 = a.pd1 + (long long)rid * kSets * CR_MAX_NP;
     const double2* pd2 = a.pd2 + (long long)rid * kSets * CR_MAX_NP;
     const int* pn = a.pd_n + rid * kSets;
-    pe_step(s, pd1, pd2, pn[0]);
-    pe_step(s, pd1, pd2, pn[0]);
-    pe_step(s, pd1 + CR_MAX_NP, pd2 + CR_MAX_NP, pn[1]);
+    pe_step(s, ring, pd1, pd2, pn[0]);
+    pe_step(s, ring, pd1, pd2, pn[0]);
+    pe_step(s, ring, pd1 + CR_MAX_NP, pd2 + CR_MAX_NP, pn[1]);
 
     const double ri = ry.zr / ry.dz;
     const int ir = (int)floor(ri);
@@ -591,6 +494,8 @@ __global__ void __launch_bounds__(kTile) march_kernel(MarchArgs a) {
 
     int set = 2;
     double rs = ry.rs;
+    const bool factored = a.S1 != nullptr && ry.ccol >= 0;
+    bool refactor = true;
     for (int rn = 0; rn < ry.nr; ++rn) {
         // updat (updat.py:38-140): bathymetry index at r + dr/2, profile indices at r
         bool reprofile = false;
@@ -614,17 +519,28 @@ __global__ void __launch_bounds__(kTile) march_kernel(MarchArgs a) {
         }
         if (reprofile) {
             assemble_rows(ry, e, ss, sb, iz_new, 0, nz + 1, a.f1, a.f2, a.f3, a.ksq);
+            refactor = true;
         } else if (iz_new != iz) {
             // only the rows that change layer
             assemble_rows(ry, e, ss, sb, iz_new, min(iz, iz_new) + 1, max(iz, iz_new), a.f1, a.f2,
                           a.f3, a.ksq);
+            refactor = true;
         }
         iz = iz_new;
         if (r >= rs) {  // stability constraints off (cupyram.py:976-999)
             set = 3;
             rs = INFINITY;
+            refactor = true;
         }
-        pe_step(s, pd1 + set * CR_MAX_NP, pd2 + set * CR_MAX_NP, pn[set]);
+        if (factored) {
+            if (refactor) {
+                factor_set(s, ring, a, ry, pd1 + set * CR_MAX_NP, pd2 + set * CR_MAX_NP, pn[set]);
+                refactor = false;
+            }
+            pe_step_fac(s, ring, a, ry, pn[set]);
+        } else {
+            pe_step(s, ring, pd1 + set * CR_MAX_NP, pd2 + set * CR_MAX_NP, pn[set]);
+        }
         r = (double)(rn + 2) * ry.dr;
         if (++mdr == ry.ndr) {
             mdr = 0;
@@ -683,6 +599,17 @@ struct cr_engine {
     double* d_tlg = nullptr;
     double2* d_cpg = nullptr;
     int* d_flags = nullptr;
+    double2 *d_S1 = nullptr, *d_S2 = nullptr, *d_S3 = nullptr, *d_AL = nullptr, *d_WF = nullptr;
+    long long fac_elems = 0;
+    // partial-fraction (sum form) march
+    bool sum_mode = false;
+    std::vector<int> tile_G;
+    std::vector<long long> tile_off;
+    std::vector<double2> pfc, pfcinf;
+    int* d_tile_G = nullptr;
+    long long* d_tile_off = nullptr;
+    double2 *d_pfc = nullptr, *d_pfcinf = nullptr;
+    double2 *d_QD = nullptr, *d_AD = nullptr, *d_WD = nullptr, *d_QU = nullptr, *d_AU = nullptr, *d_WU = nullptr;
     long long device_bytes = 0;
     bool uploaded = false, marched = false;
     cr_stats st{};
@@ -716,7 +643,9 @@ cudaError_t dev_alloc(cr_engine* e, T** p, size_t count) {
 void free_all(cr_engine* e) {
     void* ptrs[] = {e->d_rays, e->d_envs, e->d_pool, e->d_tile_ray, e->d_pd1, e->d_pd2, e->d_pd_n,
                     e->d_f1,   e->d_f2,   e->d_f3,   e->d_ksq,      e->d_u,   e->d_W,   e->d_G,
-                    e->d_tll,  e->d_cpl,  e->d_tlg,  e->d_cpg,      e->d_flags};
+                    e->d_tll,  e->d_cpl,  e->d_tlg,  e->d_cpg,      e->d_flags, e->d_S1, e->d_S2,
+                    e->d_S3,   e->d_AL,   e->d_WF,   e->d_tile_G,  e->d_tile_off, e->d_pfc, e->d_pfcinf,
+                    e->d_QD,   e->d_AD,   e->d_WD,   e->d_QU,      e->d_AU,  e->d_WU};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& ev : e->ev)
@@ -899,6 +828,38 @@ int cr_create(const cr_batch* b, cr_engine** out) {
         delete e;
         return rc;
     }
+    // The partial-fraction march needs the field's surface row to stay zero
+    // (true unless a source sits in the first depth cell); CUPYRAM_B200_SUM=0
+    // selects the product-form march.
+    {
+        const char* senv = getenv("CUPYRAM_B200_SUM");
+        bool ok = !(senv && senv[0] == '0') && b->precision == CR_PLAIN_C128;
+        for (int i = 0; ok && i < b->n_rays; ++i)
+            if ((int)std::floor(b->rays[i].zs / b->rays[i].dz) < 1) ok = false;
+        e->sum_mode = ok;
+    }
+    if (e->sum_mode) {
+        // c_inf and residues c_k of every Pade set (FP64, host)
+        e->pfc.assign((size_t)b->n_rays * kSets * CR_MAX_NP, make_double2(0.0, 0.0));
+        e->pfcinf.assign((size_t)b->n_rays * kSets, make_double2(0.0, 0.0));
+        for (int i = 0; i < b->n_rays; ++i)
+            for (int st = 0; st < kSets; ++st) {
+                const int n = e->pd_n[(size_t)i * kSets + st];
+                const double2* p1 = e->pd1.data() + ((size_t)i * kSets + st) * CR_MAX_NP;
+                const double2* p2 = e->pd2.data() + ((size_t)i * kSets + st) * CR_MAX_NP;
+                auto C = [](double2 v) { return cr::cd{v.x, v.y}; };
+                cr::cd cinf{1.0, 0.0};
+                for (int j = 0; j < n; ++j) cinf = cinf * (C(p1[j]) / C(p2[j]));
+                e->pfcinf[(size_t)i * kSets + st] = make_double2(cinf.re, cinf.im);
+                for (int k = 0; k < n; ++k) {
+                    cr::cd ck = cr::cd{1.0, 0.0} - C(p1[k]) / C(p2[k]);
+                    for (int j = 0; j < n; ++j)
+                        if (j != k)
+                            ck = ck * ((cr::cd{1.0, 0.0} - C(p1[j]) / C(p2[k])) / (cr::cd{1.0, 0.0} - C(p2[j]) / C(p2[k])));
+                    e->pfc[((size_t)i * kSets + st) * CR_MAX_NP + k] = make_double2(ck.re, ck.im);
+                }
+            }
+    }
     // tiles: rays sorted by work, longest first, 32 per tile
     std::vector<int> order(b->n_rays);
     std::iota(order.begin(), order.end(), 0);
@@ -907,15 +868,79 @@ int cr_create(const cr_batch* b, cr_engine** out) {
         const double wy = (double)(b->rays[y].nz + 2) * (b->rays[y].nr + 3);
         return wx > wy;
     });
+    if (e->sum_mode) {
+        // rays grouped by Pade order, then work; a tile holds floor(32/G) rays
+        // of G lanes each, G = the largest np in the tile
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->rays[x].np > b->rays[y].np; });
+        e->rays.resize(b->n_rays);
+        long long off = 0;
+        size_t pos = 0;
+        while (pos < order.size()) {
+            const int G = b->rays[order[pos]].np;
+            const int R = kTile / G;
+            const size_t end = std::min(order.size(), pos + (size_t)R);
+            int rows = 0;
+            for (size_t q = pos; q < end; ++q) rows = std::max(rows, b->rays[order[q]].nz + 2);
+            const int t = (int)e->tile_G.size();
+            e->tile_G.push_back(G);
+            e->tile_off.push_back(off);
+            e->tile_ray.resize((size_t)(t + 1) * kTile, -1);
+            for (size_t q = pos; q < end; ++q) {
+                const int slot = (int)(q - pos);
+                const int rid = order[q];
+                for (int k = 0; k < G; ++k) e->tile_ray[(size_t)t * kTile + slot * G + k] = rid;
+                const cr_ray& r = b->rays[rid];
+                RayDev& d = e->rays[rid];
+                d.k0 = 2.0 * M_PI * r.freq / r.c0;
+                d.omega = 2.0 * M_PI * r.freq;
+                d.c0 = r.c0;
+                d.dz = r.dz;
+                d.dr = r.dr;
+                d.zmax = r.zmax;
+                d.lyrw_lambda = r.lyrw_lambda;
+                d.attnf = r.attnf;
+                d.rs = r.rs;
+                d.zs = r.zs;
+                d.zr = r.zr;
+                d.nz = r.nz;
+                d.nr = r.nr;
+                d.np = r.np;
+                d.ndr = r.ndr;
+                d.ndz = r.ndz;
+                d.nvr = r.nvr;
+                d.nvz = r.nvz;
+                d.env = r.env;
+                d.line_off = r.line_off;
+                d.grid_off = b->compute_grids ? r.grid_off : -1;
+                d.col = off + slot;
+                d.ccol = -1;
+                d.crows = rows;
+                d.pad_ = 0;
+                e->point_updates += (double)r.nz * (double)r.nr;
+            }
+            off += (long long)rows * kTile;
+            pos = end;
+        }
+        e->n_tiles = (int)e->tile_G.size();
+        e->col_elems = off;
+        e->fac_elems = 0;
+    } else {
     e->n_tiles = (b->n_rays + kTile - 1) / kTile;
     e->tile_ray.assign((size_t)e->n_tiles * kTile, -1);
     e->rays.resize(b->n_rays);
-    long long col = 0;
+    // The factorised march stores 5 complex factors per (term, row, ray);
+    // CUPYRAM_B200_FACTOR=0 selects the on-the-fly march instead.
+    const char* fenv = getenv("CUPYRAM_B200_FACTOR");
+    const bool factored = !(fenv && fenv[0] == '0');
+    long long col = 0, fcol = 0;
     for (int t = 0; t < e->n_tiles; ++t) {
-        int rows = 0;
+        int rows = 0, npmax = 0;
         for (int l = 0; l < kTile; ++l) {
             const int k = t * kTile + l;
-            if (k < b->n_rays) rows = std::max(rows, b->rays[order[k]].nz + 2);
+            if (k < b->n_rays) {
+                rows = std::max(rows, b->rays[order[k]].nz + 2);
+                npmax = std::max(npmax, b->rays[order[k]].np);
+            }
         }
         for (int l = 0; l < kTile; ++l) {
             const int k = t * kTile + l;
@@ -946,11 +971,17 @@ int cr_create(const cr_batch* b, cr_engine** out) {
             d.line_off = r.line_off;
             d.grid_off = b->compute_grids ? r.grid_off : -1;
             d.col = col + l;
+            d.ccol = factored ? fcol + l : -1;
+            d.crows = rows;
+            d.pad_ = 0;
             e->point_updates += (double)r.nz * (double)r.nr;
         }
         col += (long long)rows * kTile;
+        if (factored) fcol += (long long)npmax * rows * kTile;
     }
     e->col_elems = col;
+    e->fac_elems = fcol;
+    }
     e->envs.resize(b->n_envs);
     for (int k = 0; k < b->n_envs; ++k) {
         const cr_env& v = b->envs[k];
@@ -969,18 +1000,36 @@ int cr_create(const cr_batch* b, cr_engine** out) {
     if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_pd1, e->pd1.size());
     if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_pd2, e->pd2.size());
     if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_pd_n, e->pd_n.size());
-    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_f1, (size_t)col);
-    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_f2, (size_t)col);
-    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_f3, (size_t)col);
-    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_ksq, (size_t)col);
-    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_u, (size_t)col);
-    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_W, (size_t)col);
-    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_G, (size_t)col);
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_f1, (size_t)e->col_elems);
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_f2, (size_t)e->col_elems);
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_f3, (size_t)e->col_elems);
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_ksq, (size_t)e->col_elems);
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_u, (size_t)e->col_elems);
+    if (ce == cudaSuccess && !e->sum_mode) ce = dev_alloc(e, &e->d_W, (size_t)e->col_elems);
+    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_G, (size_t)e->col_elems);
+    if (e->sum_mode) {
+        double2** lanecols[] = {&e->d_QD, &e->d_AD, &e->d_WD, &e->d_QU, &e->d_AU, &e->d_WU};
+        for (double2** pp : lanecols)
+            if (ce == cudaSuccess) ce = dev_alloc(e, pp, (size_t)e->col_elems);
+        if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tile_G, e->tile_G.size());
+        if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tile_off, e->tile_off.size());
+        if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_pfc, e->pfc.size());
+        if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_pfcinf, e->pfcinf.size());
+    }
     if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tll, (size_t)e->line_len);
     if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_cpl, (size_t)e->line_len);
     if (ce == cudaSuccess && e->compute_grids) ce = dev_alloc(e, &e->d_tlg, (size_t)e->grid_len);
     if (ce == cudaSuccess && e->compute_grids) ce = dev_alloc(e, &e->d_cpg, (size_t)e->grid_len);
     if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_flags, (size_t)e->n_rays);
+    if (e->fac_elems > 0) {
+        if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_S1, (size_t)e->fac_elems);
+        if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_S2, (size_t)e->fac_elems);
+        if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_S3, (size_t)e->fac_elems);
+        if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_AL, (size_t)e->fac_elems);
+        if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_WF, (size_t)e->fac_elems);
+    }
+    if (ce == cudaSuccess)
+        ce = cudaFuncSetAttribute(march_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRingBytes);
     if (ce != cudaSuccess) {
         set_global_error("cr_create: %s", cudaGetErrorString(ce));
         const int code = ce == cudaErrorMemoryAllocation ? CR_ENOMEM : CR_ECUDA;
@@ -1026,6 +1075,12 @@ int cr_upload(cr_engine* e) {
     cp(e->d_pd1, e->pd1.data(), e->pd1.size() * sizeof(double2));
     cp(e->d_pd2, e->pd2.data(), e->pd2.size() * sizeof(double2));
     cp(e->d_pd_n, e->pd_n.data(), e->pd_n.size() * sizeof(int));
+    if (e->sum_mode) {
+        cp(e->d_tile_G, e->tile_G.data(), e->tile_G.size() * sizeof(int));
+        cp(e->d_tile_off, e->tile_off.data(), e->tile_off.size() * sizeof(long long));
+        cp(e->d_pfc, e->pfc.data(), e->pfc.size() * sizeof(double2));
+        cp(e->d_pfcinf, e->pfcinf.data(), e->pfcinf.size() * sizeof(double2));
+    }
     if (ce == cudaSuccess) ce = cudaEventRecord(e->ev[1], e->stream);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
     if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
@@ -1063,11 +1118,51 @@ int cr_march(cr_engine* e) {
     a.cpg = e->d_cpg;
     a.flags = e->d_flags;
     a.compute_grids = e->compute_grids;
+    a.S1 = e->d_S1;
+    a.S2 = e->d_S2;
+    a.S3 = e->d_S3;
+    a.AL = e->d_AL;
+    a.WF = e->d_WF;
     float ms = 0.f;
-    if (ce == cudaSuccess) ce = cudaEventRecord(e->ev[0], e->stream);
-    if (ce == cudaSuccess) {
-        march_kernel<<<e->n_tiles, kTile, 0, e->stream>>>(a);
-        ce = cudaGetLastError();
+    if (ce == cudaSuccess && e->sum_mode) {
+        crk::SumArgs sa;
+        sa.rays = e->d_rays;
+        sa.tile_ray = e->d_tile_ray;
+        sa.tile_G = e->d_tile_G;
+        sa.tile_off = e->d_tile_off;
+        sa.envs = e->d_envs;
+        sa.pool = e->d_pool;
+        sa.pd1 = e->d_pd1;
+        sa.pd2 = e->d_pd2;
+        sa.pd_n = e->d_pd_n;
+        sa.pfc = e->d_pfc;
+        sa.pfcinf = e->d_pfcinf;
+        sa.f1 = e->d_f1;
+        sa.f2 = e->d_f2;
+        sa.f3 = e->d_f3;
+        sa.ksq = e->d_ksq;
+        sa.u = e->d_u;
+        sa.G = e->d_G;
+        sa.QD = e->d_QD;
+        sa.AD = e->d_AD;
+        sa.WD = e->d_WD;
+        sa.QU = e->d_QU;
+        sa.AU = e->d_AU;
+        sa.WU = e->d_WU;
+        sa.tll = e->d_tll;
+        sa.cpl = e->d_cpl;
+        sa.tlg = e->d_tlg;
+        sa.cpg = e->d_cpg;
+        sa.flags = e->d_flags;
+        sa.compute_grids = e->compute_grids;
+        ce = cudaEventRecord(e->ev[0], e->stream);
+        if (ce == cudaSuccess) ce = crk::launch_march_sum(sa, e->n_tiles, e->stream);
+    } else if (ce == cudaSuccess) {
+        ce = cudaEventRecord(e->ev[0], e->stream);
+        if (ce == cudaSuccess) {
+            march_kernel<<<e->n_tiles, kTile, kRingBytes, e->stream>>>(a);
+            ce = cudaGetLastError();
+        }
     }
     if (ce == cudaSuccess) ce = cudaEventRecord(e->ev[1], e->stream);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
@@ -1273,6 +1368,9 @@ __global__ void static_setup_kernel(const cr_ray* raw, int n_rays, int compute_g
     d.line_off = r.line_off;
     d.grid_off = compute_grids ? r.grid_off : -1;
     d.col = (long long)(b / kTile) * rows * kTile + (b % kTile);
+    d.ccol = -1;  // the static path marches on the fly (no factor arrays)
+    d.crows = rows;
+    d.pad_ = 0;
     rays[b] = d;
     flags[b] = 0;
     double2* p1 = pd1 + (size_t)b * kSets * CR_MAX_NP;
@@ -1384,8 +1482,11 @@ extern "C" int cr_march_static(const cr_batch* b, const cr_outputs* out, void* s
     a.cpg = b->compute_grids ? (double2*)out->cpg : nullptr;
     a.flags = (int*)(base + L.flags);
     a.compute_grids = b->compute_grids;
+    a.S1 = a.S2 = a.S3 = a.AL = a.WF = nullptr;
+    if (ce == cudaSuccess)
+        ce = cudaFuncSetAttribute(march_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRingBytes);
     if (ce == cudaSuccess) {
-        march_kernel<<<L.n_tiles, kTile, 0, st>>>(a);
+        march_kernel<<<L.n_tiles, kTile, kRingBytes, st>>>(a);
         ce = cudaGetLastError();
     }
     if (ce == cudaSuccess) {

@@ -19,7 +19,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "libram_oracle.so"
-MODES = {"ref": 0, "plain": 1, "f64": 2, "sim": 3}
+MODES = {"ref": 0, "plain": 1, "f64": 2, "sim": 3, "sum": 4}
 _lib = None
 
 

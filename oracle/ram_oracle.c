@@ -26,6 +26,11 @@
  *          engine's plain complex128 form.
  *   F64    everything FP64 (environment too): the FP64 oracle of the
  *          precision study.
+ *   SUM    PLAIN arithmetic with each range step in partial-fraction (sum)
+ *          form: prod_j (1 + pd1_j X)/(1 + pd2_j X) = c_inf + sum_k c_k/(1 + pd2_k X),
+ *          i.e. u_new = c_inf u + sum_k c_k (M + pd2_k D)^{-1} M u.  Same
+ *          rational operator as the product form; used to check the engine's
+ *          sum-form march against the product form.
  *   SIM    REF plus the scalar promotions of Numba's CUDA simulator under
  *          NumPy 2 (a Python float times a float32 stays float32), which is
  *          how the golden fixtures were produced: the Galerkin c1..c3 are
@@ -49,6 +54,7 @@
 #define ORACLE_PLAIN 1
 #define ORACLE_F64 2
 #define ORACLE_SIM 3
+#define ORACLE_SUM 4
 
 typedef double complex cd;
 
@@ -423,6 +429,45 @@ static void march_step(ray_state* s, int n, const cd* pd1, const cd* pd2) {
     }
 }
 
+/* One range step in partial-fraction form (see ORACLE_SUM). */
+static void march_step_sum(ray_state* s, int n, const cd* pd1, const cd* pd2) {
+    const int nz = s->nz;
+    cd cinf = 1.0;
+    for (int j = 0; j < n; ++j) cinf *= pd1[j] / pd2[j];
+    cd* mu = (cd*)malloc(sizeof(cd) * (size_t)(nz + 2));
+    cd* acc = (cd*)malloc(sizeof(cd) * (size_t)(nz + 2));
+    cd* x = (cd*)malloc(sizeof(cd) * (size_t)(nz + 2));
+    const double a1 = s->k0 * s->k0 / 6.0, a2 = 2.0 * s->k0 * s->k0 / 3.0;
+    for (int i = 1; i <= nz; ++i) {
+        mu[i] = a1 * (s->u[i - 1] + s->u[i + 1]) + a2 * s->u[i];
+        acc[i] = cinf * s->u[i];
+    }
+    for (int k = 0; k < n; ++k) {
+        cd ck = 1.0 - pd1[k] / pd2[k];
+        for (int j = 0; j < n; ++j)
+            if (j != k) ck *= (1.0 - pd1[j] / pd2[k]) / (1.0 - pd2[j] / pd2[k]);
+        const cd zero = 0.0;
+        cd r[3], q[3];
+        /* Thomas on (M + pd2_k D) x = M u */
+        galerkin(s, 1, zero, pd2[k], r, q);
+        s->up[1] = r[2] / r[1];
+        s->rs[1] = mu[1] / r[1];
+        for (int i = 2; i <= nz; ++i) {
+            galerkin(s, i, zero, pd2[k], r, q);
+            const cd den = r[1] - r[0] * s->up[i - 1];
+            s->up[i] = r[2] / den;
+            s->rs[i] = (mu[i] - r[0] * s->rs[i - 1]) / den;
+        }
+        x[nz] = s->rs[nz];
+        for (int i = nz - 1; i >= 1; --i) x[i] = s->rs[i] - s->up[i] * x[i + 1];
+        for (int i = 1; i <= nz; ++i) acc[i] += ck * x[i];
+    }
+    for (int i = 1; i <= nz; ++i) s->u[i] = acc[i];
+    free(mu);
+    free(acc);
+    free(x);
+}
+
 /* updat (updat.py:38-140): returns 1 when the profiles must be re-interpolated. */
 static int updat(ray_state* s, double r) {
     int need = 0;
@@ -562,9 +607,15 @@ static int run_ray(const cr_batch* b, int ib, int mode, double* tll_all, double*
     for (int j = 0; j < CR_MAX_NP; ++j) { pd1[j] = 0.0; pd2[j] = 0.0; }
     pd2[0] = -1.0;
     const int nself = (mode == ORACLE_REF || mode == ORACLE_SIM) ? np : 1;
-    march_step(&s, nself, pd1, pd2);
-    march_step(&s, nself, pd1, pd2);
-    march_step(&s, np, sp1, sp2);
+    if (mode == ORACLE_SUM) {
+        march_step_sum(&s, 1, pd1, pd2);
+        march_step_sum(&s, 1, pd1, pd2);
+        march_step_sum(&s, np, sp1, sp2);
+    } else {
+        march_step(&s, nself, pd1, pd2);
+        march_step(&s, nself, pd1, pd2);
+        march_step(&s, np, sp1, sp2);
+    }
 
     int mdr = 0, tlc = -1;
     double r = s.dr;
@@ -579,7 +630,8 @@ static int run_ray(const cr_batch* b, int ib, int mode, double* tll_all, double*
             rs_lim = INFINITY;
         }
         init_profiles(&s);
-        march_step(&s, np, mp1, mp2);
+        if (mode == ORACLE_SUM) march_step_sum(&s, np, mp1, mp2);
+        else march_step(&s, np, mp1, mp2);
         r = (double)(rn + 2) * s.dr;
         outpt(&s, ry, r, &mdr, &tlc, tll, cpl, tlg, cpg);
     }

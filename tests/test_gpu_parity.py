@@ -76,3 +76,28 @@ def test_no_grid_still_computes_line(cuda_device):
     res = CuPyRAM(*args, compute_grids=False, **kw).run()
     assert res["TL Grid"] is None and res["CP Grid"] is None
     assert np.abs(res["TL Line"] - fx["tl_line"]).max() <= TOL_REF
+
+
+@pytest.mark.parametrize("name", ["ram_v15", "ragged_batch", "wedge_switch"])
+def test_product_form_kernel_vs_oracle(cuda_device, monkeypatch, name):
+    """The product-form march (used when a source sits in the first depth cell)."""
+    monkeypatch.setenv("CUPYRAM_B200_SUM", "0")
+    b, _ = _batch(name)
+    with Engine(b) as eng:
+        out = eng.run()
+    ref = oracle.run(b, "plain")
+    n = b.line_len
+    assert np.abs(out["tll"][:n] - ref["tll"][:n]).max() < TOL_ORACLE
+
+
+def test_surface_source_falls_back_to_product_form(cuda_device):
+    """zs < dz puts the source in the surface row; the engine must still match."""
+    args, kw, _ = load_case("pekeris_small")
+    args = list(args)
+    args[1] = 2.0  # zs = 2 m < dz = 3 m
+    envs, p, zs, zr, pr = B.prepare(*args, dict(kw))
+    b = B.build_batch(envs, p, zs, zr, pr, False)
+    with Engine(b) as eng:
+        out = eng.run()
+    ref = oracle.run(b, "plain")
+    assert np.abs(out["tll"][:b.line_len] - ref["tll"][:b.line_len]).max() < TOL_ORACLE
