@@ -604,10 +604,12 @@ struct cr_engine {
     // partial-fraction (sum form) march
     bool sum_mode = false;
     std::vector<int> tile_G;
-    std::vector<long long> tile_off;
+    std::vector<long long> tile_off, tile_loff;
+    long long lane_elems = 0;
     std::vector<double2> pfc, pfcinf;
     int* d_tile_G = nullptr;
     long long* d_tile_off = nullptr;
+    long long* d_tile_loff = nullptr;
     double2 *d_pfc = nullptr, *d_pfcinf = nullptr;
     double2 *d_QD = nullptr, *d_AD = nullptr, *d_WD = nullptr, *d_QU = nullptr, *d_AU = nullptr, *d_WU = nullptr;
     long long device_bytes = 0;
@@ -644,7 +646,7 @@ void free_all(cr_engine* e) {
     void* ptrs[] = {e->d_rays, e->d_envs, e->d_pool, e->d_tile_ray, e->d_pd1, e->d_pd2, e->d_pd_n,
                     e->d_f1,   e->d_f2,   e->d_f3,   e->d_ksq,      e->d_u,   e->d_W,   e->d_G,
                     e->d_tll,  e->d_cpl,  e->d_tlg,  e->d_cpg,      e->d_flags, e->d_S1, e->d_S2,
-                    e->d_S3,   e->d_AL,   e->d_WF,   e->d_tile_G,  e->d_tile_off, e->d_pfc, e->d_pfcinf,
+                    e->d_S3,   e->d_AL,   e->d_WF,   e->d_tile_G,  e->d_tile_off, e->d_tile_loff, e->d_pfc, e->d_pfcinf,
                     e->d_QD,   e->d_AD,   e->d_WD,   e->d_QU,      e->d_AU,  e->d_WU};
     for (void* p : ptrs)
         if (p) cudaFree(p);
@@ -833,10 +835,16 @@ int cr_create(const cr_batch* b, cr_engine** out) {
     // selects the product-form march.
     {
         const char* senv = getenv("CUPYRAM_B200_SUM");
-        bool ok = !(senv && senv[0] == '0') && b->precision == CR_PLAIN_C128;
+        bool ok = !(senv && senv[0] == '0');
         for (int i = 0; ok && i < b->n_rays; ++i)
             if ((int)std::floor(b->rays[i].zs / b->rays[i].dz) < 1) ok = false;
         e->sum_mode = ok;
+    }
+    if (b->precision == CR_CHOSEN_C64R && !e->sum_mode) {
+        set_global_error("cr_create: the chosen complex64 form needs every source below the first depth cell "
+                         "(zs >= dz) and the partial-fraction march (CUPYRAM_B200_SUM != 0)");
+        delete e;
+        return CR_EINVAL;
     }
     if (e->sum_mode) {
         // c_inf and residues c_k of every Pade set (FP64, host)
@@ -876,7 +884,8 @@ int cr_create(const cr_batch* b, cr_engine** out) {
         long long off = 0;
         size_t pos = 0;
         while (pos < order.size()) {
-            const int G = b->rays[order[pos]].np;
+            // lanes per ray: each lane carries kT terms of the tile's largest np
+            const int G = (b->rays[order[pos]].np + crk::kT - 1) / crk::kT;
             const int R = kTile / G;
             const size_t end = std::min(order.size(), pos + (size_t)R);
             int rows = 0;
@@ -884,6 +893,8 @@ int cr_create(const cr_batch* b, cr_engine** out) {
             const int t = (int)e->tile_G.size();
             e->tile_G.push_back(G);
             e->tile_off.push_back(off);
+            e->tile_loff.push_back(e->lane_elems);
+            e->lane_elems += (long long)crk::kT * rows * kTile;
             e->tile_ray.resize((size_t)(t + 1) * kTile, -1);
             for (size_t q = pos; q < end; ++q) {
                 const int slot = (int)(q - pos);
@@ -1006,11 +1017,12 @@ int cr_create(const cr_batch* b, cr_engine** out) {
     if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_ksq, (size_t)e->col_elems);
     if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_u, (size_t)e->col_elems);
     if (ce == cudaSuccess && !e->sum_mode) ce = dev_alloc(e, &e->d_W, (size_t)e->col_elems);
-    if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_G, (size_t)e->col_elems);
+    if (ce == cudaSuccess && !e->sum_mode) ce = dev_alloc(e, &e->d_G, (size_t)e->col_elems);
     if (e->sum_mode) {
-        double2** lanecols[] = {&e->d_QD, &e->d_AD, &e->d_WD, &e->d_QU, &e->d_AU, &e->d_WU};
+        double2** lanecols[] = {&e->d_QD, &e->d_AD, &e->d_WD, &e->d_QU, &e->d_AU, &e->d_WU, &e->d_G};
         for (double2** pp : lanecols)
-            if (ce == cudaSuccess) ce = dev_alloc(e, pp, (size_t)e->col_elems);
+            if (ce == cudaSuccess) ce = dev_alloc(e, pp, (size_t)e->lane_elems);
+        if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tile_loff, e->tile_loff.size());
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tile_G, e->tile_G.size());
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tile_off, e->tile_off.size());
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_pfc, e->pfc.size());
@@ -1078,6 +1090,7 @@ int cr_upload(cr_engine* e) {
     if (e->sum_mode) {
         cp(e->d_tile_G, e->tile_G.data(), e->tile_G.size() * sizeof(int));
         cp(e->d_tile_off, e->tile_off.data(), e->tile_off.size() * sizeof(long long));
+        cp(e->d_tile_loff, e->tile_loff.data(), e->tile_loff.size() * sizeof(long long));
         cp(e->d_pfc, e->pfc.data(), e->pfc.size() * sizeof(double2));
         cp(e->d_pfcinf, e->pfcinf.data(), e->pfcinf.size() * sizeof(double2));
     }
@@ -1130,6 +1143,7 @@ int cr_march(cr_engine* e) {
         sa.tile_ray = e->d_tile_ray;
         sa.tile_G = e->d_tile_G;
         sa.tile_off = e->d_tile_off;
+        sa.tile_loff = e->d_tile_loff;
         sa.envs = e->d_envs;
         sa.pool = e->d_pool;
         sa.pd1 = e->d_pd1;
@@ -1156,7 +1170,11 @@ int cr_march(cr_engine* e) {
         sa.flags = e->d_flags;
         sa.compute_grids = e->compute_grids;
         ce = cudaEventRecord(e->ev[0], e->stream);
-        if (ce == cudaSuccess) ce = crk::launch_march_sum(sa, e->n_tiles, e->stream);
+        sa.tile_begin = 0;
+        int nl = 0;
+        if (ce == cudaSuccess)
+            ce = crk::launch_march_sum(sa, e->tile_G.data(), e->n_tiles, e->precision == CR_CHOSEN_C64R, e->stream, &nl);
+        e->st.kernel_launches = nl;
     } else if (ce == cudaSuccess) {
         ce = cudaEventRecord(e->ev[0], e->stream);
         if (ce == cudaSuccess) {
@@ -1169,7 +1187,7 @@ int cr_march(cr_engine* e) {
     if (ce == cudaSuccess) ce = cudaEventElapsedTime(&ms, e->ev[0], e->ev[1]);
     if (ce != cudaSuccess) return e->cuda_fail(ce, "cr_march");
     e->st.march_ms = ms;
-    e->st.kernel_launches = 1;
+    if (!e->sum_mode) e->st.kernel_launches = 1;
     std::vector<int> fl(e->n_rays);
     ce = cudaMemcpy(fl.data(), e->d_flags, fl.size() * sizeof(int), cudaMemcpyDeviceToHost);
     if (ce != cudaSuccess) return e->cuda_fail(ce, "cr_march (flags)");

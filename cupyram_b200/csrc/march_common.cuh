@@ -280,6 +280,18 @@ __device__ __forceinline__ void cp8(void* dst, const void* src) {
 __device__ __forceinline__ void cp4(void* dst, const void* src) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
 }
+// Zero-filling variants: when `on` is false no global byte is read and the
+// destination is filled with zeros (src-size operand 0), so a copy can be
+// issued unconditionally from branch-free code (src must still be a valid
+// address; callers clamp it).
+__device__ __forceinline__ void cp16z(void* dst, const void* src, bool on) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(on ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp8z(void* dst, const void* src, bool on) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(on ? 8 : 0)
+                 : "memory");
+}
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_wait() {

@@ -5,22 +5,27 @@
 // wavenumber rows; cupyram/fused_kernel.py:20-69):
 //
 //     P(X) = prod_j (1 + pd1_j X) / (1 + pd2_j X)          (reference: product form)
-//          = c_inf + sum_k c_k / (1 + pd2_k X)             (here: partial fractions)
+//          = c_inf + sum_j c_j / (1 + pd2_j X)             (here: partial fractions)
 //
-// so u_new = c_inf u + sum_k c_k x_k with (M + pd2_k D) x_k = M u.  The np
-// tridiagonal solves of a step are independent: one lane per term.  A warp
-// holds floor(32/G) rays x G terms (G = largest np of its tile).
+// so u_new = c_inf u + sum_j c_j x_j with (M + pd2_j D) x_j = M u: the np
+// tridiagonal solves of a step are independent.  Each lane carries kT = 2
+// terms (two independent recurrence chains per row); a ray uses
+// P = ceil(np / kT) lanes and a warp holds floor(32 / P) rays.
 //
 // Per range step each lane runs ONE pass over its column:
-//   * the back-substitution of the previous step's solve for its term,
-//   * the combination of the G terms of its ray into u_new for the row
-//     (shared memory, double-buffered, one __syncwarp of the ray's lanes),
-//   * the elimination of the next step's solve one row behind,
-// alternating the pass direction every step.  The Thomas factorisation of
-// each term (1/den, the coupling factor and w per row, both directions) is
+//   * the back-substitution of the previous step's solves of its terms,
+//   * the combination u_new = c_inf u_old + sum_j c_j x_j for the row: each
+//     lane sums its terms, the ray's P lanes exchange their sums by shuffles
+//     and add them in a fixed order (FP64, identical in every lane),
+//   * the elimination of the next step's solves two rows behind, so that the
+//     exchange latency is off the elimination's path,
+// alternating the pass direction every step.  Every lane of a warp visits
+// the same row index at the same iteration (the warp's deepest ray sets the
+// count), so the warp runs in lockstep.  The Thomas factorisation of each
+// term (1/den, the coupling factor and w per row, both directions) is
 // computed once per change of the operator - profiles, bathymetry index or
-// Pade set - and streamed from HBM, together with the lane's workspace g,
-// through a per-lane cp.async prefetch ring.
+// Pade set - and streamed from HBM, with the workspace g, through a per-lane
+// cp.async prefetch ring.
 //
 // The sum form is the reference's rational operator rearranged; on the
 // golden cases it matches the product form to <= 5e-8 dB (oracle mode "sum").
@@ -33,80 +38,147 @@ namespace crk {
 
 namespace {
 
-constexpr int kSR = 8;       // prefetch depth (rows) per lane
-constexpr int kSFields = 5;  // 16-byte fields per ring slot
+constexpr int kSR = 8;                // prefetch depth (rows) per lane
+constexpr int kFields = 1 + 4 * kT;   // u, then (W, G, Q, A) per term slot
 static_assert((kSR & (kSR - 1)) == 0, "kSR must be a power of two");
 
 struct SumSmem {
-    double2 q[kSR][kSFields][kTile];
-    double2 red[2][kTile];
+    double2 q[kSR][kFields][kTile];
 };
 
 enum SumPass { kElimOnly = 0, kFusedP = 1, kBackOnly = 2, kFactor = 3 };
 
+// Sweep precision: plain = complex128 factors / workspace and FP64
+// recurrences; chosen = complex64 factors / workspace and FP32 recurrences.
+// The factorisation itself, the combination of the terms and the stored
+// field stay FP64 / complex128 in both forms.
+template <typename R>
+struct Prec;
+template <>
+struct Prec<double> {
+    using V = double2;
+    __device__ static __forceinline__ V mk(double2 v) { return v; }
+    __device__ static __forceinline__ double2 up(V v) { return v; }
+};
+template <>
+struct Prec<float> {
+    using V = float2;
+    __device__ static __forceinline__ V mk(double2 v) { return make_float2((float)v.x, (float)v.y); }
+    __device__ static __forceinline__ double2 up(V v) { return make_double2((double)v.x, (double)v.y); }
+};
+
+template <typename R>
+__device__ __forceinline__ void cpv(void* dst, const void* src) {
+    if (sizeof(R) == 8) cp16(dst, src);
+    else cp8(dst, src);
+}
+template <typename R>
+__device__ __forceinline__ void cpvz(void* dst, const void* src, bool on) {
+    if (sizeof(R) == 8) cp16z(dst, src, on);
+    else cp8z(dst, src, on);
+}
+
 struct Lane {
-    int lane, k, gbase, G;
-    unsigned gmask;
-    long long rcol;  // ray column base (f1..f3, ksq, u)
-    long long lcol;  // lane column base (G, factors)
+    int lane, k, gbase, P;  // k: lane index within the ray's P lanes
+    int rows;               // iterations per pass, common to the warp (its deepest ray's nz + 2)
+    unsigned gmask;         // lanes of this ray
+    unsigned wmask;         // active lanes of the warp: every pass runs in lockstep over them
+    long long rcol;         // ray column base (f1..f3, ksq, u)
+    long long lcol;         // lane column base of term slot 0 (G and the factors)
+    long long lstride;      // elements between term slots of a lane column
 };
 
 struct Ops {
     int nz;
     double cfact, a1, a2;
-    double2 pole;   // pd2 of this lane's term in the active set
-    double2 ck;     // partial-fraction residue of this lane's term (0 for unused lanes)
-    double2 cinf;   // c_inf of the ray for the active set
+    double2 pole[kT];  // pd2 of this lane's terms in the active set
+    double2 ck[kT];    // partial-fraction residues (0 for slots without a term)
+    double2 cinf;      // c_inf of the ray for the active set
 };
+
+template <typename R>
+__device__ __forceinline__ const typename Prec<R>::V* fac(const double2* p) {
+    return reinterpret_cast<const typename Prec<R>::V*>(p);
+}
+template <typename R>
+__device__ __forceinline__ typename Prec<R>::V* facw(double2* p) {
+    return reinterpret_cast<typename Prec<R>::V*>(p);
+}
 
 __device__ __forceinline__ float* sfl(SumSmem& S, int slot, int lane) { return (float*)&S.q[slot][0][lane]; }
 __device__ __forceinline__ float2* sks(SumSmem& S, int slot, int lane) { return (float2*)&S.q[slot][1][lane]; }
 
-template <int PASS, bool DOWN>
+// Stream row of iteration k: the same for every lane of the warp.
+template <bool DOWN>
+__device__ __forceinline__ int row_of(const Lane& L, int k) {
+    return DOWN ? k : L.rows - 1 - k;
+}
+
+// Copies for stream row r of a factor pass (one commit group, empty outside
+// the lane's rows).
+template <typename R, int PASS, bool DOWN>
 __device__ __forceinline__ void sum_issue(const SumArgs& a, const Lane& L, SumSmem& S, int slot, int r, int nz) {
     if (r >= 0 && r <= nz + 1) {
         const long long ro = L.rcol + (long long)r * kTile;
-        const long long lo = L.lcol + (long long)r * kTile;
-        if (PASS == kFactor) {
-            float* f = sfl(S, slot, L.lane);
-            cp4(f + 0, a.f1 + ro);
-            cp4(f + 1, a.f2 + ro);
-            cp4(f + 2, a.f3 + ro);
-            cp8(sks(S, slot, L.lane), a.ksq + ro);
-        } else {
-            if (PASS == kElimOnly) cp16(&S.q[slot][0][L.lane], a.u + ro);
-            else {
-                // back-substitution of a solve eliminated in the other direction
-                cp16(&S.q[slot][0][L.lane], (DOWN ? a.WU : a.WD) + lo);
-                cp16(&S.q[slot][1][L.lane], a.G + lo);
-                cp16(&S.q[slot][4][L.lane], a.u + ro);
-            }
-            const int m = DOWN ? r - 1 : r + 1;
-            if (PASS != kBackOnly && m >= 1 && m <= nz) {
-                const long long mo = L.lcol + (long long)m * kTile;
-                cp16(&S.q[slot][2][L.lane], (DOWN ? a.QD : a.QU) + mo);
-                cp16(&S.q[slot][3][L.lane], (DOWN ? a.AD : a.AU) + mo);
-            }
+        float* f = sfl(S, slot, L.lane);
+        cp4(f + 0, a.f1 + ro);
+        cp4(f + 1, a.f2 + ro);
+        cp4(f + 2, a.f3 + ro);
+        cp8(sks(S, slot, L.lane), a.ksq + ro);
+    }
+    cp_commit();
+}
+
+// Copies for stream row r of a solve pass, branch-free: copies of rows
+// outside the lane's column are issued with zero source size (no global
+// read; the slot is zero-filled).  The elimination works two rows behind the
+// stream (row m = r -/+ 2).
+template <typename R, int PASS, bool DOWN>
+__device__ __forceinline__ void solve_issue(const SumArgs& a, const Lane& L, SumSmem& S, int slot, int r, int nz) {
+    const bool on = (r >= 0) & (r <= nz + 1);
+    const long long rr = on ? r : 0;
+    const long long ro = L.rcol + rr * kTile;
+    if (PASS == kElimOnly) cp16z(&S.q[slot][0][L.lane], a.u + ro, on);
+    else cp16z(&S.q[slot][0][L.lane], a.u + ro, on & (L.k == 0));
+    const int m = DOWN ? r - 2 : r + 2;
+    const bool mon = on & (m >= 1) & (m <= nz);
+    const long long mm = mon ? m : 0;
+#pragma unroll
+    for (int t = 0; t < kT; ++t) {
+        const long long lo = L.lcol + t * L.lstride + rr * kTile;
+        const long long mo = L.lcol + t * L.lstride + mm * kTile;
+        if (PASS != kElimOnly) {
+            // back-substitution of solves eliminated in the other direction
+            cpvz<R>(&S.q[slot][1 + 4 * t][L.lane], fac<R>(DOWN ? a.WU : a.WD) + lo, on);
+            cpvz<R>(&S.q[slot][2 + 4 * t][L.lane], fac<R>(a.G) + lo, on);
+        }
+        if (PASS != kBackOnly) {
+            cpvz<R>(&S.q[slot][3 + 4 * t][L.lane], fac<R>(DOWN ? a.QD : a.QU) + mo, mon);
+            cpvz<R>(&S.q[slot][4 + 4 * t][L.lane], fac<R>(DOWN ? a.AD : a.AU) + mo, mon);
         }
     }
     cp_commit();
 }
 
-// Thomas factorisation of (M + pole D) for this lane's term, both directions.
-template <bool DOWN>
+// Thomas factorisation of (M + pole_t D) for this lane's terms, one direction.
+template <typename R, bool DOWN>
 __device__ void sum_factor(const SumArgs& a, const Lane& L, SumSmem& S, const Ops& o) {
+    using P = Prec<R>;
     const int nz = o.nz;
     __threadfence_block();
 #pragma unroll 1
-    for (int k = 0; k < kSR; ++k) sum_issue<kFactor, DOWN>(a, L, S, k, DOWN ? k : nz + 1 - k, nz);
+    for (int k = 0; k < kSR; ++k) sum_issue<R, kFactor, DOWN>(a, L, S, k, row_of<DOWN>(L, k), nz);
     EnvRow em{}, ec{}, ep{};
-    double2 wp = c2(0.0, 0.0);
-    double2* Q = DOWN ? a.QD : a.QU;
-    double2* A = DOWN ? a.AD : a.AU;
-    double2* W = DOWN ? a.WD : a.WU;
+    double2 wp[kT];
+#pragma unroll
+    for (int t = 0; t < kT; ++t) wp[t] = c2(0.0, 0.0);
+    typename P::V* Q = facw<R>(DOWN ? a.QD : a.QU);
+    typename P::V* A = facw<R>(DOWN ? a.AD : a.AU);
+    typename P::V* W = facw<R>(DOWN ? a.WD : a.WU);
+    int seen = 0;  // rows of this lane already streamed
 #pragma unroll 1
-    for (int k = 0; k < nz + 2; ++k) {
-        const int r = DOWN ? k : nz + 1 - k;
+    for (int k = 0; k < L.rows; ++k) {
+        const int r = row_of<DOWN>(L, k);  // rows outside 0..nz+1: idle iterations
         const int slot = k & (kSR - 1);
         cp_wait<kSR - 1>();
         EnvRow er;
@@ -117,7 +189,8 @@ __device__ void sum_factor(const SumArgs& a, const Lane& L, SumSmem& S, const Op
             er.f3 = f[2];
             er.k = *sks(S, slot, L.lane);
         }
-        sum_issue<kFactor, DOWN>(a, L, S, slot, DOWN ? k + kSR : nz + 1 - k - kSR, nz);
+        sum_issue<R, kFactor, DOWN>(a, L, S, slot, row_of<DOWN>(L, k + kSR), nz);
+        if (r < 0 || r > nz + 1) continue;
         if (DOWN) {
             em = ec;
             ec = ep;
@@ -127,96 +200,164 @@ __device__ void sum_factor(const SumArgs& a, const Lane& L, SumSmem& S, const Op
             ec = em;
             em = er;
         }
-        if (k < 2) continue;
+        if (++seen < 3) continue;
         const int m = DOWN ? r - 1 : r + 1;
         if (m < 1 || m > nz) continue;
         const Drow d = galerkin3(em, ec, ep, o.cfact);
-        const double2 r1 = caxpd(o.a1, o.pole, d.d1), r2 = caxpd(o.a2, o.pole, d.d2),
-                      r3 = caxpd(o.a1, o.pole, d.d3);
-        const double2 cin = DOWN ? r1 : r3, cout = DOWN ? r3 : r1;
-        const double2 q = crcp(cfms(r2, cin, wp));
-        wp = cmul(cout, q);
-        const double2 ci = cmul(cin, q);
-        const long long mo = L.lcol + (long long)m * kTile;
-        Q[mo] = q;
-        A[mo] = c2(-ci.x, -ci.y);
-        W[mo] = wp;
+#pragma unroll
+        for (int t = 0; t < kT; ++t) {
+            const double2 r1 = caxpd(o.a1, o.pole[t], d.d1), r2 = caxpd(o.a2, o.pole[t], d.d2),
+                          r3 = caxpd(o.a1, o.pole[t], d.d3);
+            const double2 cin = DOWN ? r1 : r3, cout = DOWN ? r3 : r1;
+            const double2 q = crcp(cfms(r2, cin, wp[t]));
+            wp[t] = cmul(cout, q);
+            const double2 ci = cmul(cin, q);
+            const long long mo = L.lcol + t * L.lstride + (long long)m * kTile;
+            Q[mo] = P::mk(q);
+            A[mo] = P::mk(c2(-ci.x, -ci.y));
+            W[mo] = P::mk(wp[t]);
+        }
     }
     cp_wait<0>();
 }
 
+// g_m = q (M u)_m + al g_{m-/+1} for every term slot of the lane.
+template <typename R>
+__device__ __forceinline__ void elim_row(const Ops& o, double2 h3, double2 h2, double2 h1,
+                                         const typename Prec<R>::V* fq, const typename Prec<R>::V* fa,
+                                         typename Prec<R>::V* gp) {
+    const double2 mud = c2(fma(o.a1, h3.x + h1.x, o.a2 * h2.x), fma(o.a1, h3.y + h1.y, o.a2 * h2.y));
+    const R mx = (R)mud.x, my = (R)mud.y;
+#pragma unroll
+    for (int t = 0; t < kT; ++t) {
+        const R tx = fma(fq[t].x, mx, -fq[t].y * my), ty = fma(fq[t].x, my, fq[t].y * mx);
+        typename Prec<R>::V g;
+        g.x = fma(fa[t].x, gp[t].x, fma(-fa[t].y, gp[t].y, tx));
+        g.y = fma(fa[t].x, gp[t].y, fma(fa[t].y, gp[t].x, ty));
+        gp[t] = g;
+    }
+}
+
 // One solve pass.  kElimOnly: eliminate from the stored field u.  kFusedP:
-// back-substitute the pending solve, combine the terms into u_new (stored),
-// eliminate the next solve.  kBackOnly: back-substitute and combine only.
-template <int PASS, bool DOWN>
+// back-substitute the pending solves, combine the terms into u_new (stored
+// by lane 0 of the ray), eliminate the next solves.  kBackOnly:
+// back-substitute and combine only.  Rows are streamed in the pass
+// direction; the elimination of row m = r -/+ 2 uses u_new of rows m-1, m,
+// m+1, all finished in earlier iterations, and is placed first in the loop
+// body so that its arithmetic overlaps the latency of this row's exchange.
+// The body is branch-free (selects and predicated stores) so that the
+// compiler can interleave the independent chains.
+template <typename R, int P, int PASS, bool DOWN>
 __device__ void sum_pass(const SumArgs& a, const Lane& L, SumSmem& S, const Ops& o) {
+    using V = typename Prec<R>::V;
     const int nz = o.nz;
     __threadfence_block();
-    __syncwarp(L.gmask);
+    __syncwarp(L.wmask);
 #pragma unroll 1
-    for (int k = 0; k < kSR; ++k) sum_issue<PASS, DOWN>(a, L, S, k, DOWN ? k : nz + 1 - k, nz);
+    for (int k = 0; k < kSR; ++k) solve_issue<R, PASS, DOWN>(a, L, S, k, row_of<DOWN>(L, k), nz);
     const double2 zero = c2(0.0, 0.0);
-    double2 u0 = zero, u1 = zero, u2 = zero;  // u window, oldest first
-    double2 xp = zero;                         // back-substitution carry
-    double2 gp = zero;                         // elimination carry
+    const R zr = R(0);
+    double2 h1 = zero, h2 = zero, h3 = zero;  // u_new of the last three rows (h1 newest)
+    V xp[kT], gp[kT];
+#pragma unroll
+    for (int t = 0; t < kT; ++t) {
+        xp[t] = {zr, zr};
+        gp[t] = {zr, zr};
+    }
+    V* G = facw<R>(a.G);
+    const bool lead = (L.k == 0);
 #pragma unroll 1
-    for (int k = 0; k < nz + 2; ++k) {
-        const int r = DOWN ? k : nz + 1 - k;
+    for (int k = 0; k < L.rows; ++k) {
+        const int r = row_of<DOWN>(L, k);
         const int slot = k & (kSR - 1);
         cp_wait<kSR - 1>();
-        const double2 f0 = S.q[slot][0][L.lane];
-        double2 f1v = zero, fq = zero, fa = zero, fu = zero;
-        if (PASS != kElimOnly) {
-            f1v = S.q[slot][1][L.lane];
-            fu = S.q[slot][4][L.lane];
+        const double2 fu = S.q[slot][0][L.lane];
+        V fw[kT], fg[kT], fq[kT], fa[kT];
+#pragma unroll
+        for (int t = 0; t < kT; ++t) {
+            fw[t] = *reinterpret_cast<const V*>(&S.q[slot][1 + 4 * t][L.lane]);
+            fg[t] = *reinterpret_cast<const V*>(&S.q[slot][2 + 4 * t][L.lane]);
+            fq[t] = *reinterpret_cast<const V*>(&S.q[slot][3 + 4 * t][L.lane]);
+            fa[t] = *reinterpret_cast<const V*>(&S.q[slot][4 + 4 * t][L.lane]);
         }
+        solve_issue<R, PASS, DOWN>(a, L, S, slot, row_of<DOWN>(L, k + kSR), nz);
+        const bool valid = (r >= 0) & (r <= nz + 1);
+        const bool interior = (r >= 1) & (r <= nz);
         if (PASS != kBackOnly) {
-            fq = S.q[slot][2][L.lane];
-            fa = S.q[slot][3][L.lane];
+            // eliminate row m = r -/+ 2; (h3, h2, h1) = (u_{m-/+1}, u_m, u_{m+/-1})
+            const int m = DOWN ? r - 2 : r + 2;
+            const bool mvalid = valid & (m >= 1) & (m <= nz);
+            V g[kT];
+#pragma unroll
+            for (int t = 0; t < kT; ++t) g[t] = gp[t];
+            elim_row<R>(o, h3, h2, h1, fq, fa, g);
+            const long long mo = (long long)(mvalid ? m : 0) * kTile;
+#pragma unroll
+            for (int t = 0; t < kT; ++t) {
+                if (mvalid) G[L.lcol + t * L.lstride + mo] = g[t];
+                gp[t].x = mvalid ? g[t].x : gp[t].x;
+                gp[t].y = mvalid ? g[t].y : gp[t].y;
+            }
         }
-        sum_issue<PASS, DOWN>(a, L, S, slot, DOWN ? k + kSR : nz + 1 - k - kSR, nz);
-        const bool interior = (r >= 1 && r <= nz);
         double2 un;
         if (PASS == kElimOnly) {
-            un = interior ? f0 : zero;
+            un = interior ? fu : zero;
         } else {
-            // back-substitution: x_r = g_r - w_r x_{r-/+1}
-            double2 x = zero;
-            if (interior) {
-                const bool first = DOWN ? (r == 1) : (r == nz);
-                x = first ? f1v : c2(fma(-f0.x, xp.x, fma(f0.y, xp.y, f1v.x)), fma(-f0.x, xp.y, fma(-f0.y, xp.x, f1v.y)));
+            // back-substitution x_r = g_r - w_r x_{r-/+1} of each term, then
+            // this lane's share c_inf u_old (lane 0) + sum_t c_t x_t in FP64
+            const bool first = DOWN ? (r == 1) : (r == nz);
+            double2 v = cmul(o.cinf, fu);  // fu is zero-filled except in lane 0
+#pragma unroll
+            for (int t = 0; t < kT; ++t) {
+                V x;
+                x.x = fma(-fw[t].x, xp[t].x, fma(fw[t].y, xp[t].y, fg[t].x));
+                x.y = fma(-fw[t].x, xp[t].y, fma(-fw[t].y, xp[t].x, fg[t].y));
+                x.x = first ? fg[t].x : x.x;
+                x.y = first ? fg[t].y : x.y;
+                x.x = interior ? x.x : zr;
+                x.y = interior ? x.y : zr;
+                xp[t] = x;
+                const double2 xd = Prec<R>::up(x);
+                v = c2(fma(o.ck[t].x, xd.x, fma(-o.ck[t].y, xd.y, v.x)), fma(o.ck[t].x, xd.y, fma(o.ck[t].y, xd.x, v.y)));
             }
-            xp = x;
-            // combine the G terms of the ray: u_new = c_inf u_old + sum_k c_k x_k
-            double2* red = S.red[k & 1];
-            red[L.lane] = cmul(o.ck, x);
-            __syncwarp(L.gmask);
-            double2 acc = cmul(o.cinf, fu);
-            for (int j = 0; j < L.G; ++j) {
-                const double2 v = red[L.gbase + j];
-                acc.x += v.x;
-                acc.y += v.y;
+            // the ray's P shares, added in lane order (identical in every lane)
+            double2 sh[P];
+#pragma unroll
+            for (int j = 0; j < P; ++j) {
+                sh[j].x = __shfl_sync(L.wmask, v.x, L.gbase + j);
+                sh[j].y = __shfl_sync(L.wmask, v.y, L.gbase + j);
             }
-            un = interior ? acc : zero;
-            if (interior && L.k == 0) a.u[L.rcol + (long long)r * kTile] = un;
+            double2 tot = sh[0];
+#pragma unroll
+            for (int j = 1; j < P; ++j) {
+                tot.x += sh[j].x;
+                tot.y += sh[j].y;
+            }
+            un = interior ? tot : zero;
+            if (interior & lead) a.u[L.rcol + (long long)(interior ? r : 0) * kTile] = un;
         }
-        if (PASS == kBackOnly) continue;
-        u0 = u1;
-        u1 = u2;
-        u2 = un;
-        if (k < 2) continue;
-        const int m = DOWN ? r - 1 : r + 1;
-        if (m < 1 || m > nz) continue;
-        // (M u)_m = a1 (u_{m-1} + u_{m+1}) + a2 u_m, then g_m = q (M u)_m + al g_{m-/+1}
-        const double2 mu = c2(fma(o.a1, u0.x + u2.x, o.a2 * u1.x), fma(o.a1, u0.y + u2.y, o.a2 * u1.y));
-        const double2 t = cmul(fq, mu);
-        const double2 g = c2(fma(fa.x, gp.x, fma(-fa.y, gp.y, t.x)), fma(fa.x, gp.y, fma(fa.y, gp.x, t.y)));
-        gp = g;
-        a.G[L.lcol + (long long)m * kTile] = g;
+        h3 = valid ? h2 : h3;
+        h2 = valid ? h1 : h2;
+        h1 = valid ? un : h1;
+    }
+    // The last row to eliminate (m = nz DOWN, m = 1 UP) would need stream row
+    // nz+2 / -1; its window (u_{m-1}, u_m, u_{m+1}) is already in the history.
+    if (PASS != kBackOnly) {
+        const int m = DOWN ? nz : 1;
+        V fq[kT], fa[kT];
+#pragma unroll
+        for (int t = 0; t < kT; ++t) {
+            const long long mo = L.lcol + t * L.lstride + (long long)m * kTile;
+            fq[t] = fac<R>(DOWN ? a.QD : a.QU)[mo];
+            fa[t] = fac<R>(DOWN ? a.AD : a.AU)[mo];
+        }
+        elim_row<R>(o, h3, h2, h1, fq, fa, gp);
+#pragma unroll
+        for (int t = 0; t < kT; ++t) G[L.lcol + t * L.lstride + (long long)m * kTile] = gp[t];
     }
     cp_wait<0>();
     __threadfence_block();
-    __syncwarp(L.gmask);
+    __syncwarp(L.wmask);
 }
 
 // TL line / grid and CP line / grid of the field stored in the ray column.
@@ -249,39 +390,52 @@ __device__ void sum_outputs(const SumArgs& a, const RayDev& ry, const Lane& L, i
     }
 }
 
+// Poles and residues of this lane's term slots (term j = k + t P) in a set.
 __device__ void set_ops(const SumArgs& a, int rid, int set, const Lane& L, Ops* o) {
     const int n = a.pd_n[rid * kSets + set];
     const long long base = ((long long)rid * kSets + set) * CR_MAX_NP;
-    const int kk = L.k < n ? L.k : 0;  // unused lanes solve a copy of term 0 with weight 0
-    o->pole = a.pd2[base + kk];
-    o->ck = L.k < n ? a.pfc[base + kk] : c2(0.0, 0.0);
+#pragma unroll
+    for (int t = 0; t < kT; ++t) {
+        const int j = L.k + t * L.P;
+        // slots without a term solve a copy of term 0 with weight 0
+        o->pole[t] = a.pd2[base + (j < n ? j : 0)];
+        o->ck[t] = j < n ? a.pfc[base + j] : c2(0.0, 0.0);
+    }
     o->cinf = a.pfcinf[(long long)rid * kSets + set];
 }
 
+template <typename R>
 __device__ void sum_refactor(const SumArgs& a, const Lane& L, SumSmem& S, const Ops& o) {
-    sum_factor<true>(a, L, S, o);
-    sum_factor<false>(a, L, S, o);
+    sum_factor<R, true>(a, L, S, o);
+    sum_factor<R, false>(a, L, S, o);
     __threadfence_block();
-    __syncwarp(L.gmask);
+    __syncwarp(L.wmask);
 }
 
 }  // namespace
 
+template <typename R, int P>
 __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SumSmem& S = *reinterpret_cast<SumSmem*>(smem_raw);
-    const int t = blockIdx.x;
+    const int t = a.tile_begin + blockIdx.x;
     Lane L;
     L.lane = threadIdx.x;
-    L.G = a.tile_G[t];
+    L.P = P;
     const int rid = a.tile_ray[t * kTile + L.lane];
-    if (rid < 0 || L.G < 1) return;
-    L.k = L.lane % L.G;
+    L.wmask = __ballot_sync(0xffffffffu, rid >= 0);
+    if (rid < 0 || a.tile_G[t] != P) return;
+    L.k = L.lane % L.P;
     L.gbase = L.lane - L.k;
-    L.gmask = (L.G >= 32 ? 0xffffffffu : ((1u << L.G) - 1u)) << L.gbase;
+    L.gmask = (L.P >= 32 ? 0xffffffffu : ((1u << L.P) - 1u)) << L.gbase;
     const RayDev ry = a.rays[rid];
     L.rcol = ry.col;
-    L.lcol = a.tile_off[t] + L.lane;
+    L.lcol = a.tile_loff[t] + L.lane;
+    // the warp marches in lockstep: every pass covers the deepest ray's rows,
+    // the step loop the longest ray's steps
+    L.rows = (int)__reduce_max_sync(L.wmask, (unsigned)(ry.nz + 2));
+    L.lstride = (long long)L.rows * kTile;
+    const int nr_max = (int)__reduce_max_sync(L.wmask, (unsigned)ry.nr);
     const EnvPtrs e = env_ptrs(a.envs[ry.env], a.pool);
     const int nz = ry.nz;
     int flag = 0;
@@ -294,12 +448,12 @@ __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
     // initial profiles, split over the ray's lanes (cupyram.py:571-608, profl)
     int iz = max(1, min(nz - 1, (int)floor(e.zb[0] / ry.dz)));
     int ss = 0, sb = 0, bt = 0;
-    for (int i = L.k; i <= nz + 1; i += L.G) {
+    for (int i = L.k; i <= nz + 1; i += L.P) {
         assemble_rows(ry, e, ss, sb, iz, i, i, a.f1, a.f2, a.f3, a.ksq);
         a.u[L.rcol + (long long)i * kTile] = c2(0.0, 0.0);
     }
     __threadfence_block();
-    __syncwarp(L.gmask);
+    __syncwarp(L.wmask);
     // self-starter delta (cupyram.py:1008-1022)
     if (L.k == 0) {
         const double si = ry.zs / ry.dz;
@@ -317,17 +471,18 @@ __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
         }
     }
     __threadfence_block();
-    __syncwarp(L.gmask);
+    __syncwarp(L.wmask);
 
     const double ri = ry.zr / ry.dz;
     const int ir = (int)floor(ri);
     const double dir = ri - ir;
     int mdr = 0, tlc = -1;
 
-    // the solve "pending" back-substitution: its direction and the range /
-    // output of the step it belongs to
-    bool pend_down = true;    // direction of the pending elimination
-    bool pend_out = false;    // the pending step is followed by an outpt call
+    // The step whose back-substitution is pending (warp-uniform direction);
+    // pend_valid is per ray: false once a ray has emitted its last step.
+    bool pend_down = true;
+    bool pend_valid = false;
+    bool pend_out = false;
     double pend_r = 0.0;
 
     auto emit = [&](double r_out) {
@@ -337,25 +492,34 @@ __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
             sum_outputs(a, ry, L, tlc, r_out, ir, dir, &flag);
         }
     };
+    auto finish_pending = [&]() {  // after a pass that back-substituted the pending step
+        if (pend_valid && pend_out) emit(pend_r);
+        pend_valid = false;
+        __syncwarp(L.wmask);
+    };
     auto back_only = [&]() {
-        if (pend_down) sum_pass<kBackOnly, false>(a, L, S, o);
-        else sum_pass<kBackOnly, true>(a, L, S, o);
-        if (pend_out) emit(pend_r);
+        if (pend_down) sum_pass<R, P, kBackOnly, false>(a, L, S, o);
+        else sum_pass<R, P, kBackOnly, true>(a, L, S, o);
+        finish_pending();
     };
 
     // self-starter: two steps of 1/(1-X), one of the ip=2 operator
     set_ops(a, rid, 0, L, &o);
-    sum_refactor(a, L, S, o);
-    sum_pass<kElimOnly, true>(a, L, S, o);
+    sum_refactor<R>(a, L, S, o);
+    sum_pass<R, P, kElimOnly, true>(a, L, S, o);
     pend_down = true;
+    pend_valid = true;
     pend_out = false;
-    sum_pass<kFusedP, false>(a, L, S, o);  // back-substitute step 1, eliminate step 2 (UP)
+    sum_pass<R, P, kFusedP, false>(a, L, S, o);  // back-substitute step 1, eliminate step 2 (UP)
+    finish_pending();
     pend_down = false;
+    pend_valid = true;
     back_only();
     set_ops(a, rid, 1, L, &o);
-    sum_refactor(a, L, S, o);
-    sum_pass<kElimOnly, true>(a, L, S, o);
+    sum_refactor<R>(a, L, S, o);
+    sum_pass<R, P, kElimOnly, true>(a, L, S, o);
     pend_down = true;
+    pend_valid = true;
     pend_out = true;
     pend_r = ry.dr;  // first output at r = dr (cupyram.py:703)
 
@@ -363,60 +527,71 @@ __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
     double rs = ry.rs;
     double r = ry.dr;
     bool first_march = true;
-    for (int rn = 0; rn < ry.nr; ++rn) {
+    for (int rn = 0; rn < nr_max; ++rn) {
+        const bool live = rn < ry.nr;
         // updat (updat.py:38-140) for the step about to be taken
         bool reprofile = false;
         int iz_new = iz;
-        if (e.n_bt > 1) {
-            while (bt < e.n_bt - 1 && r >= e.rb[bt + 1]) ++bt;
-            const int b1 = min(bt + 1, e.n_bt - 1);
-            const double r0 = e.rb[bt], r1 = e.rb[b1], z0 = e.zb[bt], z1 = e.zb[b1];
-            const double zc = (b1 == bt) ? z0 : z0 + (r + 0.5 * ry.dr - r0) * (z1 - z0) / (r1 - r0);
-            iz_new = max(1, min(nz - 1, (int)floor(zc / ry.dz)));
-        }
-        if (e.n_rss > 1) {
-            const int o2 = ss;
-            while (ss < e.n_rss - 1 && r >= e.rp_ss[ss + 1]) ++ss;
-            reprofile |= (ss != o2);
-        }
-        if (e.n_rsb > 1) {
-            const int o2 = sb;
-            while (sb < e.n_rsb - 1 && r >= e.rp_sb[sb + 1]) ++sb;
-            reprofile |= (sb != o2);
-        }
-        bool change = first_march || reprofile || iz_new != iz;
         int new_set = set;
-        if (r >= rs) {  // stability constraints off (cupyram.py:976-999)
-            new_set = 3;
-            rs = INFINITY;
-            change = true;
+        bool change = false;
+        if (live) {
+            if (e.n_bt > 1) {
+                while (bt < e.n_bt - 1 && r >= e.rb[bt + 1]) ++bt;
+                const int b1 = min(bt + 1, e.n_bt - 1);
+                const double r0 = e.rb[bt], r1 = e.rb[b1], z0 = e.zb[bt], z1 = e.zb[b1];
+                const double zc = (b1 == bt) ? z0 : z0 + (r + 0.5 * ry.dr - r0) * (z1 - z0) / (r1 - r0);
+                iz_new = max(1, min(nz - 1, (int)floor(zc / ry.dz)));
+            }
+            if (e.n_rss > 1) {
+                const int o2 = ss;
+                while (ss < e.n_rss - 1 && r >= e.rp_ss[ss + 1]) ++ss;
+                reprofile |= (ss != o2);
+            }
+            if (e.n_rsb > 1) {
+                const int o2 = sb;
+                while (sb < e.n_rsb - 1 && r >= e.rp_sb[sb + 1]) ++sb;
+                reprofile |= (sb != o2);
+            }
+            if (r >= rs) {  // stability constraints off (cupyram.py:976-999)
+                new_set = 3;
+                rs = INFINITY;
+            }
+            change = first_march || reprofile || iz_new != iz || new_set != set;
         }
         const double r_out = (double)(rn + 2) * ry.dr;
-        if (change) {
+        if (__any_sync(L.wmask, change)) {
+            // some ray of the warp changes its operator: finish the pending
+            // step alone, rebuild where needed, start this step from u
             back_only();
-            if (reprofile) {
-                for (int i = L.k; i <= nz + 1; i += L.G) assemble_rows(ry, e, ss, sb, iz_new, i, i, a.f1, a.f2, a.f3, a.ksq);
-            } else if (iz_new != iz) {
-                const int lo = min(iz, iz_new) + 1, hi = max(iz, iz_new);
-                for (int i = lo + L.k; i <= hi; i += L.G) assemble_rows(ry, e, ss, sb, iz_new, i, i, a.f1, a.f2, a.f3, a.ksq);
+            if (change) {
+                if (reprofile) {
+                    for (int i = L.k; i <= nz + 1; i += L.P) assemble_rows(ry, e, ss, sb, iz_new, i, i, a.f1, a.f2, a.f3, a.ksq);
+                } else if (iz_new != iz) {
+                    const int lo = min(iz, iz_new) + 1, hi = max(iz, iz_new);
+                    for (int i = lo + L.k; i <= hi; i += L.P) assemble_rows(ry, e, ss, sb, iz_new, i, i, a.f1, a.f2, a.f3, a.ksq);
+                }
+                __threadfence_block();
+                __syncwarp(L.gmask);
+                iz = iz_new;
+                set = new_set;
+                set_ops(a, rid, set, L, &o);
+                sum_factor<R, true>(a, L, S, o);
+                sum_factor<R, false>(a, L, S, o);
+                __threadfence_block();
             }
-            __threadfence_block();
-            __syncwarp(L.gmask);
-            iz = iz_new;
-            set = new_set;
-            set_ops(a, rid, set, L, &o);
-            sum_refactor(a, L, S, o);
-            sum_pass<kElimOnly, true>(a, L, S, o);
+            __syncwarp(L.wmask);
+            sum_pass<R, P, kElimOnly, true>(a, L, S, o);
             pend_down = true;
             first_march = false;
         } else {
             // back-substitute the pending step and eliminate this one in one pass
-            if (pend_down) sum_pass<kFusedP, false>(a, L, S, o);
-            else sum_pass<kFusedP, true>(a, L, S, o);
-            if (pend_out) emit(pend_r);
+            if (pend_down) sum_pass<R, P, kFusedP, false>(a, L, S, o);
+            else sum_pass<R, P, kFusedP, true>(a, L, S, o);
+            finish_pending();
             pend_down = !pend_down;
         }
-        pend_out = true;
+        pend_valid = live;
+        pend_out = live;
         pend_r = r_out;
         r = r_out;
     }
@@ -424,12 +599,44 @@ __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
     if (L.k == 0) a.flags[rid] = flag;
 }
 
-cudaError_t launch_march_sum(const SumArgs& a, int n_tiles, cudaStream_t st) {
+template <typename R, int P>
+static cudaError_t launch_one(const SumArgs& a, int count, cudaStream_t st) {
     const size_t smem = sizeof(SumSmem);
-    cudaError_t ce = cudaFuncSetAttribute(march_sum_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t ce = cudaFuncSetAttribute(march_sum_kernel<R, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (ce != cudaSuccess) return ce;
-    march_sum_kernel<<<n_tiles, kTile, smem, st>>>(a);
+    march_sum_kernel<R, P><<<count, kTile, smem, st>>>(a);
     return cudaGetLastError();
+}
+
+template <typename R>
+static cudaError_t launch_p(const SumArgs& a, int P, int count, cudaStream_t st) {
+    switch (P) {
+        case 1: return launch_one<R, 1>(a, count, st);
+        case 2: return launch_one<R, 2>(a, count, st);
+        case 3: return launch_one<R, 3>(a, count, st);
+        case 4: return launch_one<R, 4>(a, count, st);
+        case 5: return launch_one<R, 5>(a, count, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_march_sum(const SumArgs& a0, const int* tile_P, int n_tiles, int chosen, cudaStream_t st,
+                             int* launches) {
+    // tiles are ordered by lanes per ray; one launch per run of equal P
+    int begin = 0;
+    *launches = 0;
+    while (begin < n_tiles) {
+        int end = begin + 1;
+        while (end < n_tiles && tile_P[end] == tile_P[begin]) ++end;
+        SumArgs a = a0;
+        a.tile_begin = begin;
+        const cudaError_t ce = chosen ? launch_p<float>(a, tile_P[begin], end - begin, st)
+                                      : launch_p<double>(a, tile_P[begin], end - begin, st);
+        if (ce != cudaSuccess) return ce;
+        ++*launches;
+        begin = end;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace crk

@@ -5,14 +5,18 @@
 
 namespace crk {
 
+// Pade terms carried by one lane of the sum-form march.
+constexpr int kT = 2;
+
 // Device pointers of one sum-form march.  Ray columns (f1..f3, ksq, u) and
 // lane columns (G and the factors) are stored [row][32] per tile, starting at
 // tile_off[t]; ray r of a tile uses index r, lane l of a tile uses index l.
 struct SumArgs {
     const RayDev* rays;
     const int* tile_ray;        // [n_tiles * 32]: lane -> ray, -1 unused
-    const int* tile_G;          // [n_tiles]: lanes per ray (the tile's largest np)
-    const long long* tile_off;  // [n_tiles]
+    const int* tile_G;          // [n_tiles]: lanes per ray, ceil(largest np / kT)
+    const long long* tile_off;  // [n_tiles]: ray-column base of the tile
+    const long long* tile_loff; // [n_tiles]: lane-column base (kT term slots of rows x 32)
     const EnvDev* envs;
     const double* pool;
     const double2* pd1;         // [ray][set][CR_MAX_NP]
@@ -33,8 +37,16 @@ struct SumArgs {
     double2* cpg;
     int* flags;
     int compute_grids;
+    int tile_begin;             // first tile of this launch
 };
 
-cudaError_t launch_march_sum(const SumArgs& a, int n_tiles, cudaStream_t st);
+// chosen = 1: complex64 factors / workspace, FP32 sweeps (the buffers given
+// for G and the factors are then read as float2).
+// Largest lanes-per-ray value the kernels are instantiated for (np <= 10).
+constexpr int kMaxP = 5;
+// tile_P: host copy of tile_G.  One launch per run of equal P; the number of
+// launches is returned in *launches.
+cudaError_t launch_march_sum(const SumArgs& a, const int* tile_P, int n_tiles, int chosen, cudaStream_t st,
+                             int* launches);
 
 }  // namespace crk
