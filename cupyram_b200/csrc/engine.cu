@@ -611,7 +611,7 @@ struct cr_engine {
     long long* d_tile_off = nullptr;
     long long* d_tile_loff = nullptr;
     double2 *d_pfc = nullptr, *d_pfcinf = nullptr;
-    double2 *d_QD = nullptr, *d_AD = nullptr, *d_WD = nullptr, *d_QU = nullptr, *d_AU = nullptr, *d_WU = nullptr;
+    double2 *d_QD = nullptr, *d_WD = nullptr, *d_QU = nullptr, *d_WU = nullptr, *d_ED = nullptr, *d_EU = nullptr;
     long long device_bytes = 0;
     bool uploaded = false, marched = false;
     cr_stats st{};
@@ -647,7 +647,7 @@ void free_all(cr_engine* e) {
                     e->d_f1,   e->d_f2,   e->d_f3,   e->d_ksq,      e->d_u,   e->d_W,   e->d_G,
                     e->d_tll,  e->d_cpl,  e->d_tlg,  e->d_cpg,      e->d_flags, e->d_S1, e->d_S2,
                     e->d_S3,   e->d_AL,   e->d_WF,   e->d_tile_G,  e->d_tile_off, e->d_tile_loff, e->d_pfc, e->d_pfcinf,
-                    e->d_QD,   e->d_AD,   e->d_WD,   e->d_QU,      e->d_AU,  e->d_WU};
+                    e->d_QD,   e->d_WD,   e->d_QU,   e->d_WU,      e->d_ED,  e->d_EU};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (auto& ev : e->ev)
@@ -1019,9 +1019,11 @@ int cr_create(const cr_batch* b, cr_engine** out) {
     if (ce == cudaSuccess && !e->sum_mode) ce = dev_alloc(e, &e->d_W, (size_t)e->col_elems);
     if (ce == cudaSuccess && !e->sum_mode) ce = dev_alloc(e, &e->d_G, (size_t)e->col_elems);
     if (e->sum_mode) {
-        double2** lanecols[] = {&e->d_QD, &e->d_AD, &e->d_WD, &e->d_QU, &e->d_AU, &e->d_WU, &e->d_G};
+        double2** lanecols[] = {&e->d_QD, &e->d_WD, &e->d_QU, &e->d_WU, &e->d_G};
         for (double2** pp : lanecols)
             if (ce == cudaSuccess) ce = dev_alloc(e, pp, (size_t)e->lane_elems);
+        if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_ED, (size_t)e->col_elems);
+        if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_EU, (size_t)e->col_elems);
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tile_loff, e->tile_loff.size());
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tile_G, e->tile_G.size());
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tile_off, e->tile_off.size());
@@ -1158,11 +1160,11 @@ int cr_march(cr_engine* e) {
         sa.u = e->d_u;
         sa.G = e->d_G;
         sa.QD = e->d_QD;
-        sa.AD = e->d_AD;
         sa.WD = e->d_WD;
         sa.QU = e->d_QU;
-        sa.AU = e->d_AU;
         sa.WU = e->d_WU;
+        sa.ED = e->d_ED;
+        sa.EU = e->d_EU;
         sa.tll = e->d_tll;
         sa.cpl = e->d_cpl;
         sa.tlg = e->d_tlg;

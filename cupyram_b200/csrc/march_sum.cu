@@ -25,7 +25,13 @@
 // term (1/den, the coupling factor and w per row, both directions) is
 // computed once per change of the operator - profiles, bathymetry index or
 // Pade set - and streamed from HBM, with the workspace g, through a per-lane
-// cp.async prefetch ring.
+// cp.async prefetch ring.  Only 1/den and w are stored per term; the
+// elimination's coupling factor -(a1 + pd2 e) / den is rebuilt in FP64 from
+// 1/den and the row's Galerkin coupling e (d1 going down, d3 going up,
+// complex128), which is stored once per ray row and shared by the ray's
+// terms.  The solve loop
+// handles kU rows per iteration so that one row's term exchange overlaps the
+// next row's recurrences.
 //
 // The sum form is the reference's rational operator rearranged; on the
 // golden cases it matches the product form to <= 5e-8 dB (oracle mode "sum").
@@ -39,8 +45,13 @@ namespace crk {
 namespace {
 
 constexpr int kSR = 8;                // prefetch depth (rows) per lane
-constexpr int kFields = 1 + 4 * kT;   // u, then (W, G, Q, A) per term slot
+#ifndef CR_SUM_ROWS
+#define CR_SUM_ROWS 2
+#endif
+constexpr int kU = CR_SUM_ROWS;       // rows per solve-loop iteration
+constexpr int kFields = 2 + 3 * kT;   // u, e, then (W, G, Q) per term slot
 static_assert((kSR & (kSR - 1)) == 0, "kSR must be a power of two");
+static_assert(kSR % kU == 0, "the prefetch ring must hold whole iterations");
 
 struct SumSmem {
     double2 q[kSR][kFields][kTile];
@@ -80,7 +91,9 @@ __device__ __forceinline__ void cpvz(void* dst, const void* src, bool on) {
 
 struct Lane {
     int lane, k, gbase, P;  // k: lane index within the ray's P lanes
-    int rows;               // iterations per pass, common to the warp (its deepest ray's nz + 2)
+    int rows;               // rows per lane column, common to the warp (its deepest ray's nz + 2)
+    int span;               // iterations per pass: rows rounded up to a multiple of kU
+    int nzmin;              // shallowest ray of the warp (bounds the unchecked iterations)
     unsigned gmask;         // lanes of this ray
     unsigned wmask;         // active lanes of the warp: every pass runs in lockstep over them
     long long rcol;         // ray column base (f1..f3, ksq, u)
@@ -111,7 +124,7 @@ __device__ __forceinline__ float2* sks(SumSmem& S, int slot, int lane) { return 
 // Stream row of iteration k: the same for every lane of the warp.
 template <bool DOWN>
 __device__ __forceinline__ int row_of(const Lane& L, int k) {
-    return DOWN ? k : L.rows - 1 - k;
+    return DOWN ? k : L.span - 1 - k;
 }
 
 // Copies for stream row r of a factor pass (one commit group, empty outside
@@ -129,32 +142,66 @@ __device__ __forceinline__ void sum_issue(const SumArgs& a, const Lane& L, SumSm
     cp_commit();
 }
 
-// Copies for stream row r of a solve pass, branch-free: copies of rows
-// outside the lane's column are issued with zero source size (no global
-// read; the slot is zero-filled).  The elimination works two rows behind the
-// stream (row m = r -/+ 2).
-template <typename R, int PASS, bool DOWN>
-__device__ __forceinline__ void solve_issue(const SumArgs& a, const Lane& L, SumSmem& S, int slot, int r, int nz) {
-    const bool on = (r >= 0) & (r <= nz + 1);
-    const long long rr = on ? r : 0;
-    const long long ro = L.rcol + rr * kTile;
-    if (PASS == kElimOnly) cp16z(&S.q[slot][0][L.lane], a.u + ro, on);
-    else cp16z(&S.q[slot][0][L.lane], a.u + ro, on & (L.k == 0));
-    const int m = DOWN ? r - 2 : r + 2;
-    const bool mon = on & (m >= 1) & (m <= nz);
-    const long long mm = mon ? m : 0;
+// Column pointers of one solve pass (element 0 of the lane's columns).
+template <typename R>
+struct PassPtrs {
+    using V = typename Prec<R>::V;
+    double2* u;        // field (ray column)
+    const double2* e;  // Galerkin coupling of this pass's elimination (ray column)
+    const V* w[kT];    // w of the solves being back-substituted (eliminated the other way)
+    V* g[kT];          // workspace: read by the back-substitution, rewritten by the elimination
+    const V* q[kT];    // 1/den of this pass's elimination
+};
+
+template <typename R, bool DOWN>
+__device__ __forceinline__ PassPtrs<R> pass_ptrs(const SumArgs& a, const Lane& L) {
+    PassPtrs<R> p;
+    p.u = a.u + L.rcol;
+    p.e = (DOWN ? a.ED : a.EU) + L.rcol;
 #pragma unroll
     for (int t = 0; t < kT; ++t) {
-        const long long lo = L.lcol + t * L.lstride + rr * kTile;
-        const long long mo = L.lcol + t * L.lstride + mm * kTile;
+        const long long lo = L.lcol + t * L.lstride;
+        p.w[t] = fac<R>(DOWN ? a.WU : a.WD) + lo;
+        p.g[t] = facw<R>(a.G) + lo;
+        p.q[t] = fac<R>(DOWN ? a.QD : a.QU) + lo;
+    }
+    return p;
+}
+
+// Copies for stream row r of a solve pass (one commit group).  The
+// elimination works two rows behind the stream (row m = r -/+ 2).  CHECK:
+// rows outside the lane's column are copied with zero source size (no
+// global read; the slot is zero-filled).  Without CHECK every row involved
+// is an interior row of every ray of the warp.
+template <typename R, int PASS, bool DOWN, bool CHECK>
+__device__ __forceinline__ void solve_issue(const PassPtrs<R>& p, const Lane& L, SumSmem& S, int slot, int r,
+                                            int nz) {
+    const bool on = CHECK ? ((r >= 0) & (r <= nz + 1)) : true;
+    const int ro = (CHECK ? (on ? r : 0) : r) * kTile;
+    const bool uon = PASS == kElimOnly ? on : (on & (L.k == 0));
+    if (CHECK || PASS != kElimOnly) cp16z(&S.q[slot][0][L.lane], p.u + ro, uon);
+    else cp16(&S.q[slot][0][L.lane], p.u + ro);
+    const int m = DOWN ? r - 2 : r + 2;
+    const bool mon = CHECK ? (on & (m >= 1) & (m <= nz)) : true;
+    const int mo = (CHECK ? (mon ? m : 0) : m) * kTile;
+    if (PASS != kBackOnly) {
+        if (CHECK) cp16z(&S.q[slot][1][L.lane], p.e + mo, mon);
+        else cp16(&S.q[slot][1][L.lane], p.e + mo);
+    }
+#pragma unroll
+    for (int t = 0; t < kT; ++t) {
         if (PASS != kElimOnly) {
-            // back-substitution of solves eliminated in the other direction
-            cpvz<R>(&S.q[slot][1 + 4 * t][L.lane], fac<R>(DOWN ? a.WU : a.WD) + lo, on);
-            cpvz<R>(&S.q[slot][2 + 4 * t][L.lane], fac<R>(a.G) + lo, on);
+            if (CHECK) {
+                cpvz<R>(&S.q[slot][2 + 3 * t][L.lane], p.w[t] + ro, on);
+                cpvz<R>(&S.q[slot][3 + 3 * t][L.lane], p.g[t] + ro, on);
+            } else {
+                cpv<R>(&S.q[slot][2 + 3 * t][L.lane], p.w[t] + ro);
+                cpv<R>(&S.q[slot][3 + 3 * t][L.lane], p.g[t] + ro);
+            }
         }
         if (PASS != kBackOnly) {
-            cpvz<R>(&S.q[slot][3 + 4 * t][L.lane], fac<R>(DOWN ? a.QD : a.QU) + mo, mon);
-            cpvz<R>(&S.q[slot][4 + 4 * t][L.lane], fac<R>(DOWN ? a.AD : a.AU) + mo, mon);
+            if (CHECK) cpvz<R>(&S.q[slot][4 + 3 * t][L.lane], p.q[t] + mo, mon);
+            else cpv<R>(&S.q[slot][4 + 3 * t][L.lane], p.q[t] + mo);
         }
     }
     cp_commit();
@@ -173,11 +220,11 @@ __device__ void sum_factor(const SumArgs& a, const Lane& L, SumSmem& S, const Op
 #pragma unroll
     for (int t = 0; t < kT; ++t) wp[t] = c2(0.0, 0.0);
     typename P::V* Q = facw<R>(DOWN ? a.QD : a.QU);
-    typename P::V* A = facw<R>(DOWN ? a.AD : a.AU);
+    double2* E = DOWN ? a.ED : a.EU;
     typename P::V* W = facw<R>(DOWN ? a.WD : a.WU);
     int seen = 0;  // rows of this lane already streamed
 #pragma unroll 1
-    for (int k = 0; k < L.rows; ++k) {
+    for (int k = 0; k < L.span; ++k) {
         const int r = row_of<DOWN>(L, k);  // rows outside 0..nz+1: idle iterations
         const int slot = k & (kSR - 1);
         cp_wait<kSR - 1>();
@@ -204,6 +251,7 @@ __device__ void sum_factor(const SumArgs& a, const Lane& L, SumSmem& S, const Op
         const int m = DOWN ? r - 1 : r + 1;
         if (m < 1 || m > nz) continue;
         const Drow d = galerkin3(em, ec, ep, o.cfact);
+        if (L.k == 0) E[L.rcol + (long long)m * kTile] = DOWN ? d.d1 : d.d3;
 #pragma unroll
         for (int t = 0; t < kT; ++t) {
             const double2 r1 = caxpd(o.a1, o.pole[t], d.d1), r2 = caxpd(o.a2, o.pole[t], d.d2),
@@ -211,30 +259,166 @@ __device__ void sum_factor(const SumArgs& a, const Lane& L, SumSmem& S, const Op
             const double2 cin = DOWN ? r1 : r3, cout = DOWN ? r3 : r1;
             const double2 q = crcp(cfms(r2, cin, wp[t]));
             wp[t] = cmul(cout, q);
-            const double2 ci = cmul(cin, q);
             const long long mo = L.lcol + t * L.lstride + (long long)m * kTile;
             Q[mo] = P::mk(q);
-            A[mo] = P::mk(c2(-ci.x, -ci.y));
             W[mo] = P::mk(wp[t]);
         }
     }
     cp_wait<0>();
 }
 
-// g_m = q (M u)_m + al g_{m-/+1} for every term slot of the lane.
+// g_m = q (M u)_m + al g_{m-/+1} for every term slot of the lane, with the
+// coupling factor al = -(a1 + pole e) q rebuilt from the stored 1/den q and
+// the row's Galerkin coupling e (the factorisation's own arithmetic).
 template <typename R>
-__device__ __forceinline__ void elim_row(const Ops& o, double2 h3, double2 h2, double2 h1,
-                                         const typename Prec<R>::V* fq, const typename Prec<R>::V* fa,
-                                         typename Prec<R>::V* gp) {
+__device__ __forceinline__ void elim_row(const Ops& o, double2 h3, double2 h2, double2 h1, double2 fe,
+                                         const typename Prec<R>::V* fq, typename Prec<R>::V* gp) {
     const double2 mud = c2(fma(o.a1, h3.x + h1.x, o.a2 * h2.x), fma(o.a1, h3.y + h1.y, o.a2 * h2.y));
     const R mx = (R)mud.x, my = (R)mud.y;
 #pragma unroll
     for (int t = 0; t < kT; ++t) {
+        // a1 + pole e cancels strongly for some terms: formed in FP64 like the
+        // factorisation, only al is rounded to the sweep precision
+        const double2 cin = caxpd(o.a1, o.pole[t], fe);
+        const double2 ci = cmul(cin, Prec<R>::up(fq[t]));
+        const R ax = (R)(-ci.x), ay = (R)(-ci.y);
         const R tx = fma(fq[t].x, mx, -fq[t].y * my), ty = fma(fq[t].x, my, fq[t].y * mx);
         typename Prec<R>::V g;
-        g.x = fma(fa[t].x, gp[t].x, fma(-fa[t].y, gp[t].y, tx));
-        g.y = fma(fa[t].x, gp[t].y, fma(fa[t].y, gp[t].x, ty));
+        g.x = fma(ax, gp[t].x, fma(-ay, gp[t].y, tx));
+        g.y = fma(ax, gp[t].y, fma(ay, gp[t].x, ty));
         gp[t] = g;
+    }
+}
+
+// One streamed row of a solve pass, in registers.
+template <typename R>
+struct RowF {
+    using V = typename Prec<R>::V;
+    double2 u;
+    double2 e;
+    V w[kT], g[kT], q[kT];
+};
+
+template <typename R>
+__device__ __forceinline__ void load_row(const SumSmem& S, int slot, int lane, RowF<R>& f) {
+    using V = typename Prec<R>::V;
+    f.u = S.q[slot][0][lane];
+    f.e = S.q[slot][1][lane];
+#pragma unroll
+    for (int t = 0; t < kT; ++t) {
+        f.w[t] = *reinterpret_cast<const V*>(&S.q[slot][2 + 3 * t][lane]);
+        f.g[t] = *reinterpret_cast<const V*>(&S.q[slot][3 + 3 * t][lane]);
+        f.q[t] = *reinterpret_cast<const V*>(&S.q[slot][4 + 3 * t][lane]);
+    }
+}
+
+// Carried state of a solve pass.
+template <typename R>
+struct SolveState {
+    using V = typename Prec<R>::V;
+    double2 h1, h2, h3;  // u_new of the last three rows (h1 newest)
+    V xp[kT];            // back-substitution chains
+    V gp[kT];            // elimination chains
+};
+
+// Stream row r of a solve pass.  The elimination of row m = r -/+ 2 uses
+// (h3, h2, h1) = (u_{m-/+1}, u_m, u_{m+/-1}) and comes first; then the
+// back-substitution x_r = g_r - w_r x_{r-/+1} of each term and this lane's
+// share c_inf u_old (lane 0) + sum_t c_t x_t in FP64, and the exchange of
+// the ray's P shares, added in lane order (identical in every lane).
+// CHECK: rows outside a ray's column are handled with selects and predicated
+// stores (branch-free); without CHECK, r and m are interior rows of every
+// ray of the warp and r is no ray's first back-substitution row.
+template <typename R, int P, int PASS, bool DOWN, bool CHECK>
+__device__ __forceinline__ void solve_row(const PassPtrs<R>& p, const Lane& L, const Ops& o, const RowF<R>& f,
+                                          int r, SolveState<R>& st) {
+    using V = typename Prec<R>::V;
+    const int nz = o.nz;
+    const double2 zero = c2(0.0, 0.0);
+    const R zr = R(0);
+    const bool valid = CHECK ? ((r >= 0) & (r <= nz + 1)) : true;
+    const bool interior = CHECK ? ((r >= 1) & (r <= nz)) : true;
+    if (PASS != kBackOnly) {
+        const int m = DOWN ? r - 2 : r + 2;
+        const bool mvalid = CHECK ? (valid & (m >= 1) & (m <= nz)) : true;
+        V g[kT];
+#pragma unroll
+        for (int t = 0; t < kT; ++t) g[t] = st.gp[t];
+        elim_row<R>(o, st.h3, st.h2, st.h1, f.e, f.q, g);
+        const int mo = (CHECK ? (mvalid ? m : 0) : m) * kTile;
+#pragma unroll
+        for (int t = 0; t < kT; ++t) {
+            if (mvalid) p.g[t][mo] = g[t];
+            if (CHECK) {
+                st.gp[t].x = mvalid ? g[t].x : st.gp[t].x;
+                st.gp[t].y = mvalid ? g[t].y : st.gp[t].y;
+            } else {
+                st.gp[t] = g[t];
+            }
+        }
+    }
+    double2 un;
+    if (PASS == kElimOnly) {
+        un = interior ? f.u : zero;
+    } else {
+        const bool first = CHECK ? (DOWN ? (r == 1) : (r == nz)) : false;
+        double2 v = cmul(o.cinf, f.u);  // f.u is zero-filled except in lane 0
+#pragma unroll
+        for (int t = 0; t < kT; ++t) {
+            V x;
+            x.x = fma(-f.w[t].x, st.xp[t].x, fma(f.w[t].y, st.xp[t].y, f.g[t].x));
+            x.y = fma(-f.w[t].x, st.xp[t].y, fma(-f.w[t].y, st.xp[t].x, f.g[t].y));
+            if (CHECK) {
+                x.x = first ? f.g[t].x : x.x;
+                x.y = first ? f.g[t].y : x.y;
+                x.x = interior ? x.x : zr;
+                x.y = interior ? x.y : zr;
+            }
+            st.xp[t] = x;
+            const double2 xd = Prec<R>::up(x);
+            v = c2(fma(o.ck[t].x, xd.x, fma(-o.ck[t].y, xd.y, v.x)), fma(o.ck[t].x, xd.y, fma(o.ck[t].y, xd.x, v.y)));
+        }
+        double2 sh[P];
+#pragma unroll
+        for (int j = 0; j < P; ++j) {
+            sh[j].x = __shfl_sync(L.wmask, v.x, L.gbase + j);
+            sh[j].y = __shfl_sync(L.wmask, v.y, L.gbase + j);
+        }
+        double2 tot = sh[0];
+#pragma unroll
+        for (int j = 1; j < P; ++j) {
+            tot.x += sh[j].x;
+            tot.y += sh[j].y;
+        }
+        un = interior ? tot : zero;
+        if (interior & (L.k == 0)) p.u[(CHECK ? (interior ? r : 0) : r) * kTile] = un;
+    }
+    if (CHECK) {
+        st.h3 = valid ? st.h2 : st.h3;
+        st.h2 = valid ? st.h1 : st.h2;
+        st.h1 = valid ? un : st.h1;
+    } else {
+        st.h3 = st.h2;
+        st.h2 = st.h1;
+        st.h1 = un;
+    }
+}
+
+// Iterations [k0, k1) of a solve pass, kU rows each.
+template <typename R, int P, int PASS, bool DOWN, bool CHECK>
+__device__ __forceinline__ void solve_iters(const PassPtrs<R>& p, const Lane& L, SumSmem& S, const Ops& o, int k0,
+                                            int k1, SolveState<R>& st) {
+#pragma unroll 1
+    for (int k = k0; k < k1; k += kU) {
+        cp_wait<kSR - kU>();
+        RowF<R> f[kU];
+#pragma unroll
+        for (int j = 0; j < kU; ++j) load_row<R>(S, (k + j) & (kSR - 1), L.lane, f[j]);
+#pragma unroll
+        for (int j = 0; j < kU; ++j)
+            solve_issue<R, PASS, DOWN, CHECK>(p, L, S, (k + j) & (kSR - 1), row_of<DOWN>(L, k + j + kSR), o.nz);
+#pragma unroll
+        for (int j = 0; j < kU; ++j) solve_row<R, P, PASS, DOWN, CHECK>(p, L, o, f[j], row_of<DOWN>(L, k + j), st);
     }
 }
 
@@ -242,118 +426,44 @@ __device__ __forceinline__ void elim_row(const Ops& o, double2 h3, double2 h2, d
 // back-substitute the pending solves, combine the terms into u_new (stored
 // by lane 0 of the ray), eliminate the next solves.  kBackOnly:
 // back-substitute and combine only.  Rows are streamed in the pass
-// direction; the elimination of row m = r -/+ 2 uses u_new of rows m-1, m,
-// m+1, all finished in earlier iterations, and is placed first in the loop
-// body so that its arithmetic overlaps the latency of this row's exchange.
-// The body is branch-free (selects and predicated stores) so that the
-// compiler can interleave the independent chains.
+// direction, kU per iteration.
 template <typename R, int P, int PASS, bool DOWN>
 __device__ void sum_pass(const SumArgs& a, const Lane& L, SumSmem& S, const Ops& o) {
-    using V = typename Prec<R>::V;
     const int nz = o.nz;
+    const PassPtrs<R> p = pass_ptrs<R, DOWN>(a, L);
     __threadfence_block();
     __syncwarp(L.wmask);
 #pragma unroll 1
-    for (int k = 0; k < kSR; ++k) solve_issue<R, PASS, DOWN>(a, L, S, k, row_of<DOWN>(L, k), nz);
-    const double2 zero = c2(0.0, 0.0);
-    const R zr = R(0);
-    double2 h1 = zero, h2 = zero, h3 = zero;  // u_new of the last three rows (h1 newest)
-    V xp[kT], gp[kT];
+    for (int k = 0; k < kSR; ++k) solve_issue<R, PASS, DOWN, true>(p, L, S, k, row_of<DOWN>(L, k), nz);
+    SolveState<R> st;
+    st.h1 = st.h2 = st.h3 = c2(0.0, 0.0);
 #pragma unroll
     for (int t = 0; t < kT; ++t) {
-        xp[t] = {zr, zr};
-        gp[t] = {zr, zr};
+        st.xp[t] = {R(0), R(0)};
+        st.gp[t] = {R(0), R(0)};
     }
-    V* G = facw<R>(a.G);
-    const bool lead = (L.k == 0);
-#pragma unroll 1
-    for (int k = 0; k < L.rows; ++k) {
-        const int r = row_of<DOWN>(L, k);
-        const int slot = k & (kSR - 1);
-        cp_wait<kSR - 1>();
-        const double2 fu = S.q[slot][0][L.lane];
-        V fw[kT], fg[kT], fq[kT], fa[kT];
-#pragma unroll
-        for (int t = 0; t < kT; ++t) {
-            fw[t] = *reinterpret_cast<const V*>(&S.q[slot][1 + 4 * t][L.lane]);
-            fg[t] = *reinterpret_cast<const V*>(&S.q[slot][2 + 4 * t][L.lane]);
-            fq[t] = *reinterpret_cast<const V*>(&S.q[slot][3 + 4 * t][L.lane]);
-            fa[t] = *reinterpret_cast<const V*>(&S.q[slot][4 + 4 * t][L.lane]);
-        }
-        solve_issue<R, PASS, DOWN>(a, L, S, slot, row_of<DOWN>(L, k + kSR), nz);
-        const bool valid = (r >= 0) & (r <= nz + 1);
-        const bool interior = (r >= 1) & (r <= nz);
-        if (PASS != kBackOnly) {
-            // eliminate row m = r -/+ 2; (h3, h2, h1) = (u_{m-/+1}, u_m, u_{m+/-1})
-            const int m = DOWN ? r - 2 : r + 2;
-            const bool mvalid = valid & (m >= 1) & (m <= nz);
-            V g[kT];
-#pragma unroll
-            for (int t = 0; t < kT; ++t) g[t] = gp[t];
-            elim_row<R>(o, h3, h2, h1, fq, fa, g);
-            const long long mo = (long long)(mvalid ? m : 0) * kTile;
-#pragma unroll
-            for (int t = 0; t < kT; ++t) {
-                if (mvalid) G[L.lcol + t * L.lstride + mo] = g[t];
-                gp[t].x = mvalid ? g[t].x : gp[t].x;
-                gp[t].y = mvalid ? g[t].y : gp[t].y;
-            }
-        }
-        double2 un;
-        if (PASS == kElimOnly) {
-            un = interior ? fu : zero;
-        } else {
-            // back-substitution x_r = g_r - w_r x_{r-/+1} of each term, then
-            // this lane's share c_inf u_old (lane 0) + sum_t c_t x_t in FP64
-            const bool first = DOWN ? (r == 1) : (r == nz);
-            double2 v = cmul(o.cinf, fu);  // fu is zero-filled except in lane 0
-#pragma unroll
-            for (int t = 0; t < kT; ++t) {
-                V x;
-                x.x = fma(-fw[t].x, xp[t].x, fma(fw[t].y, xp[t].y, fg[t].x));
-                x.y = fma(-fw[t].x, xp[t].y, fma(-fw[t].y, xp[t].x, fg[t].y));
-                x.x = first ? fg[t].x : x.x;
-                x.y = first ? fg[t].y : x.y;
-                x.x = interior ? x.x : zr;
-                x.y = interior ? x.y : zr;
-                xp[t] = x;
-                const double2 xd = Prec<R>::up(x);
-                v = c2(fma(o.ck[t].x, xd.x, fma(-o.ck[t].y, xd.y, v.x)), fma(o.ck[t].x, xd.y, fma(o.ck[t].y, xd.x, v.y)));
-            }
-            // the ray's P shares, added in lane order (identical in every lane)
-            double2 sh[P];
-#pragma unroll
-            for (int j = 0; j < P; ++j) {
-                sh[j].x = __shfl_sync(L.wmask, v.x, L.gbase + j);
-                sh[j].y = __shfl_sync(L.wmask, v.y, L.gbase + j);
-            }
-            double2 tot = sh[0];
-#pragma unroll
-            for (int j = 1; j < P; ++j) {
-                tot.x += sh[j].x;
-                tot.y += sh[j].y;
-            }
-            un = interior ? tot : zero;
-            if (interior & lead) a.u[L.rcol + (long long)(interior ? r : 0) * kTile] = un;
-        }
-        h3 = valid ? h2 : h3;
-        h2 = valid ? h1 : h2;
-        h1 = valid ? un : h1;
-    }
+    // Iterations whose rows r (and elimination rows, and the rows they
+    // prefetch) are interior rows of every ray of the warp, and past every
+    // first back-substitution row, run unchecked:
+    //   DOWN: 3 <= r and r + kSR <= nzmin + 1;   UP: kSR <= r <= nzmin - 2.
+    const int lb = DOWN ? 3 : L.span + 1 - L.nzmin;
+    const int ub = DOWN ? L.nzmin + 2 - kSR - kU : L.span - kU - kSR;  // last steady start
+    const int k_lo = min(L.span, (max(lb, 0) + kU - 1) / kU * kU);
+    const int k_hi = ub < k_lo ? k_lo : min(L.span, (ub / kU) * kU + kU);
+    solve_iters<R, P, PASS, DOWN, true>(p, L, S, o, 0, k_lo, st);
+    solve_iters<R, P, PASS, DOWN, false>(p, L, S, o, k_lo, k_hi, st);
+    solve_iters<R, P, PASS, DOWN, true>(p, L, S, o, k_hi, L.span, st);
     // The last row to eliminate (m = nz DOWN, m = 1 UP) would need stream row
     // nz+2 / -1; its window (u_{m-1}, u_m, u_{m+1}) is already in the history.
     if (PASS != kBackOnly) {
+        using V = typename Prec<R>::V;
         const int m = DOWN ? nz : 1;
-        V fq[kT], fa[kT];
+        V fq[kT];
 #pragma unroll
-        for (int t = 0; t < kT; ++t) {
-            const long long mo = L.lcol + t * L.lstride + (long long)m * kTile;
-            fq[t] = fac<R>(DOWN ? a.QD : a.QU)[mo];
-            fa[t] = fac<R>(DOWN ? a.AD : a.AU)[mo];
-        }
-        elim_row<R>(o, h3, h2, h1, fq, fa, gp);
+        for (int t = 0; t < kT; ++t) fq[t] = p.q[t][m * kTile];
+        elim_row<R>(o, st.h3, st.h2, st.h1, p.e[m * kTile], fq, st.gp);
 #pragma unroll
-        for (int t = 0; t < kT; ++t) G[L.lcol + t * L.lstride + (long long)m * kTile] = gp[t];
+        for (int t = 0; t < kT; ++t) p.g[t][m * kTile] = st.gp[t];
     }
     cp_wait<0>();
     __threadfence_block();
@@ -434,6 +544,8 @@ __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
     // the warp marches in lockstep: every pass covers the deepest ray's rows,
     // the step loop the longest ray's steps
     L.rows = (int)__reduce_max_sync(L.wmask, (unsigned)(ry.nz + 2));
+    L.span = (L.rows + kU - 1) / kU * kU;
+    L.nzmin = (int)__reduce_min_sync(L.wmask, (unsigned)ry.nz);
     L.lstride = (long long)L.rows * kTile;
     const int nr_max = (int)__reduce_max_sync(L.wmask, (unsigned)ry.nr);
     const EnvPtrs e = env_ptrs(a.envs[ry.env], a.pool);
@@ -485,23 +597,25 @@ __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
     bool pend_out = false;
     double pend_r = 0.0;
 
-    auto emit = [&](double r_out) {
-        if (++mdr == ry.ndr) {
-            mdr = 0;
-            ++tlc;
-            sum_outputs(a, ry, L, tlc, r_out, ir, dir, &flag);
-        }
-    };
-    auto finish_pending = [&]() {  // after a pass that back-substituted the pending step
-        if (pend_valid && pend_out) emit(pend_r);
-        pend_valid = false;
-        __syncwarp(L.wmask);
-    };
-    auto back_only = [&]() {
-        if (pend_down) sum_pass<R, P, kBackOnly, false>(a, L, S, o);
-        else sum_pass<R, P, kBackOnly, true>(a, L, S, o);
-        finish_pending();
-    };
+    // the output of the pending step is written once its back-substitution
+    // has stored the field (pass-level bookkeeping, inlined by hand so that
+    // no local escapes into a call and the lane state stays in registers)
+#define CR_FINISH_PENDING()                                                 \
+    do {                                                                    \
+        if (pend_valid && pend_out && ++mdr == ry.ndr) {                    \
+            mdr = 0;                                                        \
+            ++tlc;                                                          \
+            sum_outputs(a, ry, L, tlc, pend_r, ir, dir, &flag);             \
+        }                                                                   \
+        pend_valid = false;                                                 \
+        __syncwarp(L.wmask);                                                \
+    } while (0)
+#define CR_BACK_ONLY()                                                      \
+    do {                                                                    \
+        if (pend_down) sum_pass<R, P, kBackOnly, false>(a, L, S, o);        \
+        else sum_pass<R, P, kBackOnly, true>(a, L, S, o);                   \
+        CR_FINISH_PENDING();                                                \
+    } while (0)
 
     // self-starter: two steps of 1/(1-X), one of the ip=2 operator
     set_ops(a, rid, 0, L, &o);
@@ -511,10 +625,10 @@ __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
     pend_valid = true;
     pend_out = false;
     sum_pass<R, P, kFusedP, false>(a, L, S, o);  // back-substitute step 1, eliminate step 2 (UP)
-    finish_pending();
+    CR_FINISH_PENDING();
     pend_down = false;
     pend_valid = true;
-    back_only();
+    CR_BACK_ONLY();
     set_ops(a, rid, 1, L, &o);
     sum_refactor<R>(a, L, S, o);
     sum_pass<R, P, kElimOnly, true>(a, L, S, o);
@@ -562,7 +676,7 @@ __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
         if (__any_sync(L.wmask, change)) {
             // some ray of the warp changes its operator: finish the pending
             // step alone, rebuild where needed, start this step from u
-            back_only();
+            CR_BACK_ONLY();
             if (change) {
                 if (reprofile) {
                     for (int i = L.k; i <= nz + 1; i += L.P) assemble_rows(ry, e, ss, sb, iz_new, i, i, a.f1, a.f2, a.f3, a.ksq);
@@ -587,7 +701,7 @@ __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
             // back-substitute the pending step and eliminate this one in one pass
             if (pend_down) sum_pass<R, P, kFusedP, false>(a, L, S, o);
             else sum_pass<R, P, kFusedP, true>(a, L, S, o);
-            finish_pending();
+            CR_FINISH_PENDING();
             pend_down = !pend_down;
         }
         pend_valid = live;
@@ -595,9 +709,12 @@ __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
         pend_r = r_out;
         r = r_out;
     }
-    back_only();
+    CR_BACK_ONLY();
     if (L.k == 0) a.flags[rid] = flag;
 }
+
+#undef CR_FINISH_PENDING
+#undef CR_BACK_ONLY
 
 template <typename R, int P>
 static cudaError_t launch_one(const SumArgs& a, int count, cudaStream_t st) {
@@ -608,15 +725,13 @@ static cudaError_t launch_one(const SumArgs& a, int count, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-template <typename R>
-static cudaError_t launch_p(const SumArgs& a, int P, int count, cudaStream_t st) {
-    switch (P) {
-        case 1: return launch_one<R, 1>(a, count, st);
-        case 2: return launch_one<R, 2>(a, count, st);
-        case 3: return launch_one<R, 3>(a, count, st);
-        case 4: return launch_one<R, 4>(a, count, st);
-        case 5: return launch_one<R, 5>(a, count, st);
-        default: return cudaErrorInvalidValue;
+template <typename R, int P = 1>
+static cudaError_t launch_p(const SumArgs& a, int p, int count, cudaStream_t st) {
+    if constexpr (P > kMaxP) {
+        return cudaErrorInvalidValue;
+    } else {
+        if (p == P) return launch_one<R, P>(a, count, st);
+        return launch_p<R, P + 1>(a, p, count, st);
     }
 }
 

@@ -6,7 +6,10 @@
 namespace crk {
 
 // Pade terms carried by one lane of the sum-form march.
-constexpr int kT = 2;
+#ifndef CR_SUM_TERMS
+#define CR_SUM_TERMS 2
+#endif
+constexpr int kT = CR_SUM_TERMS;
 
 // Device pointers of one sum-form march.  Ray columns (f1..f3, ksq, u) and
 // lane columns (G and the factors) are stored [row][32] per tile, starting at
@@ -30,7 +33,8 @@ struct SumArgs {
     float2* ksq;
     double2* u;
     double2* G;
-    double2 *QD, *AD, *WD, *QU, *AU, *WU;
+    double2 *QD, *WD, *QU, *WU;  // lane columns: 1/den and w per term, both directions
+    double2 *ED, *EU;            // ray columns: Galerkin coupling into the row (d1 down, d3 up)
     double* tll;
     double2* cpl;
     double* tlg;
@@ -43,7 +47,7 @@ struct SumArgs {
 // chosen = 1: complex64 factors / workspace, FP32 sweeps (the buffers given
 // for G and the factors are then read as float2).
 // Largest lanes-per-ray value the kernels are instantiated for (np <= 10).
-constexpr int kMaxP = 5;
+constexpr int kMaxP = (10 + kT - 1) / kT;
 // tile_P: host copy of tile_G.  One launch per run of equal P; the number of
 // launches is returned in *launches.
 cudaError_t launch_march_sum(const SumArgs& a, const int* tile_P, int n_tiles, int chosen, cudaStream_t st,
