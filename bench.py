@@ -17,7 +17,19 @@ e2e   : the same march through the C ABI call cr_run with host buffers: H2D of
         the batch's inputs, the march, D2H of the TL / CP lines into pinned host
         memory, every step; host wall clock around the call.
 
+Other configurations (--config):
+  pekeris   - Pekeris waveguide, one ray: 50 Hz, zs = zr = 50 m, 100 m water
+              over a 1700 m/s bottom, rmax 10 km, dr 2 m, dz 0.25 m, np 8, TL
+              line and TL grid (ndr 1, ndz 4)
+  wedge     - uneven wedge batch, 10,000 rays: per-ray slope, bottom,
+              frequency (log-U[25,500] Hz), rmax U[5,40] km, np U{4..8},
+              dr = lambda/4, dz = lambda/8
+  precision - the Munk batch at 16,384 rays with a coarse TL grid (ndr 20,
+              ndz 100): TL errors of the chosen form against complex128 over
+              the line and the grid, cells with TL < 100 dB
+
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--form plain|chosen]
+                       [--config munk|pekeris|wedge|precision]
        python bench.py --impl reference ...   (CPU restatement on host cores)
 Multi-GPU: launch with torch.distributed.run; every rank marches its own
 seeded batch of the same size (weak scaling, no collective on the data path).
@@ -48,7 +60,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--form", choices=["plain", "chosen"], default="plain")
-    ap.add_argument("--rays", type=int, default=4096)
+    ap.add_argument("--config", choices=["munk", "pekeris", "wedge", "precision"], default="munk")
+    ap.add_argument("--rays", type=int, default=0, help="rays per GPU (0: the configuration's own count)")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-chosen", action="store_true", help="skip the chosen-form comparison")
@@ -67,15 +80,44 @@ def dist_env():
     return rank, world, local
 
 
-def workload_config(a, batch):
-    return {"workload": f"Munk deep-water batch, {a.rays} rays per GPU, per-ray f U[50,200] Hz, "
-                        "zs U[50,1000] m, SSP updates every 5 km (sigma 2 m/s, 1 km corr.), "
-                        f"{a.depth:g} m flat, rmax {a.rmax / 1000:g} km, dr 25 m, dz 1 m, np 6, zr 500 m, TL line",
-            "rays_per_gpu": int(batch.n_rays), "form": a.form, "seed": a.seed,
-            "point_updates_per_gpu": batch.point_updates,
-            "nz_range": [int(batch.rays["nz"].min()), int(batch.rays["nz"].max())],
-            "steps_per_ray": int(batch.rays["nr"][0]),
-            "l2": "working set > L2 (column arrays ~1.6 GB per 4096 rays; no flush needed)"}
+DEFAULT_RAYS = {"munk": 4096, "pekeris": 1, "wedge": 10000, "precision": 16384}
+
+
+def workload(a, rank):
+    """(batch, config dict) of the selected configuration for this rank."""
+    from cupyram_b200 import workloads
+    n = a.rays or DEFAULT_RAYS[a.config]
+    seed = a.seed + 1000 * rank
+    if a.config == "pekeris":
+        batch = workloads.build(*workloads.pekeris(), compute_grids=True)
+        desc = ("Pekeris waveguide, one ray: 50 Hz, zs = zr = 50 m, 100 m water (1500 m/s) over a "
+                "1700 m/s, 1.5 g/cm3, 0.5 dB/lambda bottom to 300 m + 10 lambda layer, rmax 10 km, "
+                "dr 2 m, dz 0.25 m, np 8, ns 1, TL line + TL grid (ndr 1, ndz 4)")
+        l2 = "working set < L2 (one ray); no flush: every step rewrites the same columns"
+    elif a.config == "wedge":
+        batch = workloads.build(*workloads.wedge_batch(n, seed=seed), compute_grids=False)
+        desc = (f"uneven wedge batch, {n} rays per GPU: depth U[50,400] m -> U[50,400] m, "
+                "cb U[1550,1800], rhob U[1.3,2.0], attn U[0.2,1.0], f log-U[25,500] Hz, rmax U[5,40] km, "
+                "dr = lambda/4, dz = lambda/8, np U{4..8}, TL line")
+        l2 = "working set > L2; no flush needed"
+    else:
+        grids = a.config == "precision"
+        args, kw = workloads.munk_batch(n, seed=seed, rmax=a.rmax, depth=a.depth)
+        if grids:
+            kw.update(ndr=20, ndz=100)
+        batch = workloads.build(args, kw, compute_grids=grids)
+        desc = (f"Munk deep-water batch, {n} rays per GPU, per-ray f U[50,200] Hz, "
+                "zs U[50,1000] m, SSP updates every 5 km (sigma 2 m/s, 1 km corr.), "
+                f"{a.depth:g} m flat, rmax {a.rmax / 1000:g} km, dr 25 m, dz 1 m, np 6, zr 500 m, TL line"
+                + (" + TL grid (ndr 20, ndz 100)" if grids else ""))
+        l2 = "working set > L2 (column arrays ~4 GB per 1000 rays); no flush needed"
+    r = batch.rays
+    cfg = {"workload": desc, "config": a.config, "rays_per_gpu": int(batch.n_rays), "form": a.form,
+           "seed": seed, "point_updates_per_gpu": batch.point_updates,
+           "nz_range": [int(r["nz"].min()), int(r["nz"].max())],
+           "steps_per_ray_range": [int(r["nr"].min()), int(r["nr"].max())],
+           "np_range": [int(r["np"].min()), int(r["np"].max())], "l2": l2}
+    return batch, cfg
 
 
 class ClockSampler:
@@ -170,12 +212,11 @@ def tl_errors(tl_ref, tl):
 
 
 def chosen_form(a, batch, out_plain, torch, world, pg, barrier, peak):
-    """Time the complex64 + FP32-sweep form on the same batch; TL error vs the plain run."""
+    """Time the complex64 + FP32-sweep form on the same batch; TL errors against the plain run."""
     from cupyram_b200.engine import Engine
-    ref = out_plain["tll"].numpy().copy()
+    refs = {k: out_plain[k].numpy().copy() for k in ("tll", "tlg") if k in out_plain}
     eng = Engine(batch, precision="chosen")
-    out = {"tll": torch.empty(batch.line_len, dtype=torch.float64, pin_memory=True),
-           "cpl": torch.empty(batch.line_len, dtype=torch.complex128, pin_memory=True)}
+    out = alloc_pinned(batch, torch)
     for _ in range(a.warmup):
         eng.run(out)
     barrier()
@@ -189,24 +230,42 @@ def chosen_form(a, batch, out_plain, torch, world, pg, barrier, peak):
         tt = torch.tensor([t], dtype=torch.float64, device="cuda")
         pg.all_reduce(tt, op=pg.ReduceOp.MAX)
         t = float(tt[0])
-    emax, erms = tl_errors(ref, out["tll"].numpy())
+    emax, erms = tl_errors(refs["tll"], out["tll"].numpy())
+    errs = {"tl_err_max_db": emax, "tl_err_rms_db": erms, "tl_err_cells": "TL line, cells with TL < 100 dB"}
+    if "tlg" in refs:
+        gmax, grms = tl_errors(refs["tlg"], out["tlg"].numpy())
+        errs.update(tl_grid_err_max_db=gmax, tl_grid_err_rms_db=grms,
+                    tl_grid_cells=int(np.sum(np.isfinite(refs["tlg"]) & (refs["tlg"] < 100.0))))
     eng.close()
     pu = batch.point_updates
     value = pu * world * a.steps / (t * 1e-3)
-    achieved = pu * B_ALG["chosen"] / (float(np.mean(ms)) * 1e-3) / 1e9
+    per_launch_s = float(np.mean(ms)) * 1e-3
+    achieved = pu * B_ALG["chosen"] / per_launch_s / 1e9
+    tpp = profiled_traffic("chosen") if a.config == "munk" else None
     return {"form": "complex64 factors and workspace, FP32 sweeps, FP64 term combination and field",
-            "value": value, "unit": UNIT, "ms_per_step": t / a.steps,
-            "tl_err_max_db": emax, "tl_err_rms_db": erms, "tl_err_cells": "TL line, cells with TL < 100 dB",
+            "value": value, "unit": UNIT, "ms_per_step": t / a.steps, **errs,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "bytes_per_point_update": B_ALG["chosen"]}}
+                         "frac": achieved / peak, "bytes_per_point_update": B_ALG["chosen"],
+                         "traffic": (tpp * pu) if tpp else None,
+                         "traffic_gbs": (tpp * pu / per_launch_s / 1e9) if tpp else None,
+                         "traffic_frac": (tpp * pu / per_launch_s / 1e9 / peak) if tpp else None}}
+
+
+def alloc_pinned(batch, torch):
+    """Pinned host output buffers of a batch (the end-to-end path's destination)."""
+    out = {"tll": torch.empty(max(batch.line_len, 1), dtype=torch.float64, pin_memory=True),
+           "cpl": torch.empty(max(batch.line_len, 1), dtype=torch.complex128, pin_memory=True)}
+    if batch.compute_grids:
+        out["tlg"] = torch.empty(max(batch.grid_len, 1), dtype=torch.float64, pin_memory=True)
+        out["cpg"] = torch.empty(max(batch.grid_len, 1), dtype=torch.complex128, pin_memory=True)
+    return out
 
 
 def run_reference(a):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    from cupyram_b200 import workloads
-    batch = workloads.build(*workloads.munk_batch(a.rays, seed=a.seed, rmax=a.rmax), compute_grids=False)
+    batch, cfg = workload(a, 0)
     vals = []
     for k in range(a.warmup + a.steps):
         v, dt, n, cores = cpu_sample(batch, a.cpu_rays, a.seed + k, "ref")
@@ -216,7 +275,7 @@ def run_reference(a):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": float(np.mean([dt for _, dt in vals]) * 1e3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
-            "data": "synthetic", "impl": "reference", "config": workload_config(a, batch),
+            "data": "synthetic", "impl": "reference", "config": cfg,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": f"{n} rays of the batch per step, one ray per core, full march "
                                        "each (the reference has no CPU path of its own: its kernels "
@@ -241,14 +300,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                 device_id=torch.device("cuda", local))
         pg = dist
-    from cupyram_b200 import workloads
     from cupyram_b200.engine import Engine
-    batch = workloads.build(*workloads.munk_batch(a.rays, seed=a.seed + 1000 * rank, rmax=a.rmax,
-                                                  depth=a.depth), compute_grids=False)
+    batch, cfg = workload(a, rank)
     eng = Engine(batch, precision=a.form)
-    # pinned host output buffers for the end-to-end path
-    out = {"tll": torch.empty(batch.line_len, dtype=torch.float64, pin_memory=True),
-           "cpl": torch.empty(batch.line_len, dtype=torch.complex128, pin_memory=True)}
+    out = alloc_pinned(batch, torch)  # pinned host output buffers for the end-to-end path
 
     def barrier():
         torch.cuda.synchronize()
@@ -294,16 +349,18 @@ def main():
         return 0
     per_launch_s = float(np.mean(march_ms)) * 1e-3
     achieved = pu * B_ALG[a.form] / per_launch_s / 1e9
-    tpp = profiled_traffic(a.form)
+    tpp = profiled_traffic(a.form) if a.config == "munk" else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": t_march / a.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
             "dtype": "complex128" if a.form == "plain" else "complex64",
-            "data": "synthetic", "config": workload_config(a, batch),
+            "data": "synthetic", "config": cfg,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "bytes_per_point_update": B_ALG[a.form],
-                         "traffic": (tpp * pu) if tpp else None},
+                         "traffic": (tpp * pu) if tpp else None,
+                         "traffic_gbs": (tpp * pu / per_launch_s / 1e9) if tpp else None,
+                         "traffic_frac": (tpp * pu / per_launch_s / 1e9 / peak) if tpp else None},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d_b),
                     "d2h_bytes_per_step": int(d2h_b)},
             "gpu_launches": int(launches), "clocks": clk.summary()}

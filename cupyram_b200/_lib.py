@@ -13,7 +13,7 @@ import numpy as np
 LIB_NAME = "libcupyram_b200.so"
 LIB_PATH = Path(__file__).resolve().parent / LIB_NAME
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 MAX_NP = 10
 
 # status codes (enum cr_status)
@@ -52,7 +52,8 @@ class CrStats(ctypes.Structure):
                 ("point_updates", ctypes.c_double), ("h2d_bytes", ctypes.c_int64),
                 ("d2h_bytes", ctypes.c_int64), ("kernel_launches", ctypes.c_int32),
                 ("rays_failed", ctypes.c_int32), ("tile_rays", ctypes.c_int32),
-                ("n_tiles", ctypes.c_int32), ("device_bytes", ctypes.c_int64)]
+                ("n_tiles", ctypes.c_int32), ("device_bytes", ctypes.c_int64),
+                ("column_rays", ctypes.c_int32), ("column_launches", ctypes.c_int32)]
 
 
 # every symbol the header declares, with its signature

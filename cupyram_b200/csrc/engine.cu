@@ -49,6 +49,7 @@
 #include <vector>
 
 #include "../../include/cupyram_b200.h"
+#include "march_col.cuh"
 #include "march_common.cuh"
 #include "march_sum.cuh"
 #include "pade.h"
@@ -612,6 +613,21 @@ struct cr_engine {
     long long* d_tile_loff = nullptr;
     double2 *d_pfc = nullptr, *d_pfcinf = nullptr;
     double2 *d_QD = nullptr, *d_WD = nullptr, *d_QU = nullptr, *d_WU = nullptr, *d_ED = nullptr, *d_EU = nullptr;
+    // column-parallel march: rays marched by one thread-block cluster each,
+    // one launch per (Pade term count) group on its own stream
+    struct ColGroup {
+        int cluster, terms, nz_max, begin, count;
+        cudaStream_t stream;
+        cudaEvent_t done;
+    };
+    std::vector<int> col_ray;
+    std::vector<ColGroup> col_groups;
+    // batched launches after the first run on their own streams
+    std::vector<cudaStream_t> sum_streams;
+    std::vector<cudaEvent_t> sum_done;
+    std::vector<int> term_capacity;  // Pade terms each ray's lanes / cluster can carry
+    int* d_col_ray = nullptr;
+    cudaEvent_t ev_fork = nullptr;
     long long device_bytes = 0;
     bool uploaded = false, marched = false;
     cr_stats st{};
@@ -647,9 +663,18 @@ void free_all(cr_engine* e) {
                     e->d_f1,   e->d_f2,   e->d_f3,   e->d_ksq,      e->d_u,   e->d_W,   e->d_G,
                     e->d_tll,  e->d_cpl,  e->d_tlg,  e->d_cpg,      e->d_flags, e->d_S1, e->d_S2,
                     e->d_S3,   e->d_AL,   e->d_WF,   e->d_tile_G,  e->d_tile_off, e->d_tile_loff, e->d_pfc, e->d_pfcinf,
-                    e->d_QD,   e->d_WD,   e->d_QU,   e->d_WU,      e->d_ED,  e->d_EU};
+                    e->d_QD,   e->d_WD,   e->d_QU,   e->d_WU,      e->d_ED,  e->d_EU, e->d_col_ray};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    for (auto& g : e->col_groups) {
+        if (g.done) cudaEventDestroy(g.done);
+        if (g.stream) cudaStreamDestroy(g.stream);
+    }
+    if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+    for (size_t i = 1; i < e->sum_streams.size(); ++i)
+        if (e->sum_streams[i]) cudaStreamDestroy(e->sum_streams[i]);
+    for (auto ev : e->sum_done)
+        if (ev) cudaEventDestroy(ev);
     for (auto& ev : e->ev)
         if (ev) cudaEventDestroy(ev);
     if (e->stream) cudaStreamDestroy(e->stream);
@@ -805,6 +830,133 @@ int cr_pade(double freq, double c0, int np, int ns, double dr, int ip, double* p
     return CR_OK;
 }
 
+namespace {
+
+// c_inf = prod_j pd1_j / pd2_j and the residues
+// c_k = (1 - pd1_k/pd2_k) prod_{j != k} (1 - pd1_j/pd2_k) / (1 - pd2_j/pd2_k)
+// of Pade set `st` of a ray: prod_j (1 + pd1_j X)/(1 + pd2_j X) = c_inf + sum_k c_k/(1 + pd2_k X).
+void partial_fractions(cr_engine* e, int ray, int st) {
+    const int n = e->pd_n[(size_t)ray * kSets + st];
+    const double2* p1 = e->pd1.data() + ((size_t)ray * kSets + st) * CR_MAX_NP;
+    const double2* p2 = e->pd2.data() + ((size_t)ray * kSets + st) * CR_MAX_NP;
+    auto C = [](double2 v) { return cr::cd{v.x, v.y}; };
+    cr::cd cinf{1.0, 0.0};
+    for (int j = 0; j < n; ++j) cinf = cinf * (C(p1[j]) / C(p2[j]));
+    e->pfcinf[(size_t)ray * kSets + st] = make_double2(cinf.re, cinf.im);
+    for (int k = 0; k < CR_MAX_NP; ++k) {
+        double2 out = make_double2(0.0, 0.0);
+        if (k < n) {
+            cr::cd ck = cr::cd{1.0, 0.0} - C(p1[k]) / C(p2[k]);
+            for (int j = 0; j < n; ++j)
+                if (j != k) ck = ck * ((cr::cd{1.0, 0.0} - C(p1[j]) / C(p2[k])) / (cr::cd{1.0, 0.0} - C(p2[j]) / C(p2[k])));
+            out = make_double2(ck.re, ck.im);
+        }
+        e->pfc[((size_t)ray * kSets + st) * CR_MAX_NP + k] = out;
+    }
+}
+
+// Device record of a ray (everything but its column placement).
+RayDev ray_dev(const cr_ray& r, bool grids) {
+    RayDev d{};
+    d.k0 = 2.0 * M_PI * r.freq / r.c0;
+    d.omega = 2.0 * M_PI * r.freq;
+    d.c0 = r.c0;
+    d.dz = r.dz;
+    d.dr = r.dr;
+    d.zmax = r.zmax;
+    d.lyrw_lambda = r.lyrw_lambda;
+    d.attnf = r.attnf;
+    d.rs = r.rs;
+    d.zs = r.zs;
+    d.zr = r.zr;
+    d.nz = r.nz;
+    d.nr = r.nr;
+    d.np = r.np;
+    d.ndr = r.ndr;
+    d.ndz = r.ndz;
+    d.nvr = r.nvr;
+    d.nvz = r.nvz;
+    d.env = r.env;
+    d.line_off = r.line_off;
+    d.grid_off = grids ? r.grid_off : -1;
+    d.ccol = -1;
+    d.pad_ = 0;
+    return d;
+}
+
+// Pade terms of a ray's largest set (the warps of its column-kernel CTAs).
+int col_terms(const std::vector<int>& pd_n, int ray) {
+    int t = 0;
+    for (int s = 0; s < kSets; ++s) t = std::max(t, pd_n[(size_t)ray * kSets + s]);
+    return t;
+}
+
+// Cluster size of each column ray.  The smallest cluster that holds the
+// column in shared memory uses the fewest SMs per ray; when the column rays
+// leave SMs idle, a ray gets up to SMs / rays CTAs (at most 16, at least 64
+// rows per slice) so that its slices, and its steps, are shorter.  Only
+// sizes whose clusters can be resident are used.
+std::vector<int> column_clusters(const cr_batch* b, const std::vector<int>& pd_n, const std::vector<char>& is_col,
+                                 bool chosen) {
+    std::vector<int> cl((size_t)b->n_rays, 0);
+    int n_col = 0;
+    for (char c : is_col) n_col += c ? 1 : 0;
+    if (n_col == 0) return cl;
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int share = std::max(1, sms / n_col);
+    std::map<std::tuple<int, int, int>, bool> runs;
+    for (int i = 0; i < b->n_rays; ++i) {
+        if (!is_col[(size_t)i]) continue;
+        const int nz = b->rays[i].nz, terms = col_terms(pd_n, i);
+        const int cmin = crk::col_cluster_size(nz, terms, chosen);
+        int C = std::max(cmin, std::min({16, share, std::max(1, nz / 64)}));
+        for (; C > cmin; --C) {
+            const auto key = std::make_tuple(C, terms, nz);
+            auto it = runs.find(key);
+            if (it == runs.end()) it = runs.emplace(key, crk::col_max_active_clusters(C, terms, nz, chosen) > 0).first;
+            if (it->second) break;
+        }
+        cl[(size_t)i] = C;
+    }
+    return cl;
+}
+
+// Rays marched by the column-parallel kernel instead of the batched one.
+// A ray's lockstep march in a batched tile takes about (nz + 2)(nr + 4)
+// row steps of one warp in sequence; when that alone exceeds the time the
+// whole batch needs at the batched kernel's throughput, the ray would set
+// the launch's length, and a cluster of SMs marches it instead.  A ray must
+// fit the shared memory of a cluster of at most 16 CTAs.  CUPYRAM_B200_COL:
+// 0 never, 1 every ray that fits, unset / other: this rule.
+std::vector<char> pick_column_rays(const cr_batch* b, const std::vector<int>& pd_n, bool chosen) {
+    constexpr double kRowStepSeconds = 0.3e-6;    // batched tile, one row of one step
+    constexpr double kUpdatesPerSecond = 1.3e10;  // batched kernel, whole GPU
+    std::vector<char> col((size_t)b->n_rays, 0);
+    const char* env = getenv("CUPYRAM_B200_COL");
+    const int mode = (env && env[0] == '0') ? 0 : ((env && env[0] == '1') ? 1 : 2);
+    if (mode == 0) return col;
+    double work = 0.0;
+    for (int i = 0; i < b->n_rays; ++i) work += (double)b->rays[i].nz * b->rays[i].nr;
+    const double tau = work / kUpdatesPerSecond;
+    std::map<std::tuple<int, int, int>, bool> runs;
+    for (int i = 0; i < b->n_rays; ++i) {
+        const cr_ray& r = b->rays[i];
+        if (mode == 2 && (double)(r.nz + 2) * (r.nr + 4) * kRowStepSeconds <= tau) continue;
+        const int terms = col_terms(pd_n, i);
+        const int cluster = crk::col_cluster_size(r.nz, terms, chosen);
+        if (cluster == 0) continue;
+        const auto key = std::make_tuple(cluster, terms, r.nz);
+        auto it = runs.find(key);
+        if (it == runs.end())
+            it = runs.emplace(key, crk::col_max_active_clusters(cluster, terms, r.nz, chosen) > 0).first;
+        if (it->second) col[(size_t)i] = 1;
+    }
+    return col;
+}
+
+}  // namespace
+
 int cr_create(const cr_batch* b, cr_engine** out) {
     if (!out) {
         set_global_error("cr_create: out is NULL");
@@ -851,22 +1003,7 @@ int cr_create(const cr_batch* b, cr_engine** out) {
         e->pfc.assign((size_t)b->n_rays * kSets * CR_MAX_NP, make_double2(0.0, 0.0));
         e->pfcinf.assign((size_t)b->n_rays * kSets, make_double2(0.0, 0.0));
         for (int i = 0; i < b->n_rays; ++i)
-            for (int st = 0; st < kSets; ++st) {
-                const int n = e->pd_n[(size_t)i * kSets + st];
-                const double2* p1 = e->pd1.data() + ((size_t)i * kSets + st) * CR_MAX_NP;
-                const double2* p2 = e->pd2.data() + ((size_t)i * kSets + st) * CR_MAX_NP;
-                auto C = [](double2 v) { return cr::cd{v.x, v.y}; };
-                cr::cd cinf{1.0, 0.0};
-                for (int j = 0; j < n; ++j) cinf = cinf * (C(p1[j]) / C(p2[j]));
-                e->pfcinf[(size_t)i * kSets + st] = make_double2(cinf.re, cinf.im);
-                for (int k = 0; k < n; ++k) {
-                    cr::cd ck = cr::cd{1.0, 0.0} - C(p1[k]) / C(p2[k]);
-                    for (int j = 0; j < n; ++j)
-                        if (j != k)
-                            ck = ck * ((cr::cd{1.0, 0.0} - C(p1[j]) / C(p2[k])) / (cr::cd{1.0, 0.0} - C(p2[j]) / C(p2[k])));
-                    e->pfc[((size_t)i * kSets + st) * CR_MAX_NP + k] = make_double2(ck.re, ck.im);
-                }
-            }
+            for (int st = 0; st < kSets; ++st) partial_fractions(e, i, st);
     }
     // tiles: rays sorted by work, longest first, 32 per tile
     std::vector<int> order(b->n_rays);
@@ -877,19 +1014,42 @@ int cr_create(const cr_batch* b, cr_engine** out) {
         return wx > wy;
     });
     if (e->sum_mode) {
-        // rays grouped by Pade order, then work; a tile holds floor(32/G) rays
-        // of G lanes each, G = the largest np in the tile
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return b->rays[x].np > b->rays[y].np; });
+        const std::vector<char> is_col = pick_column_rays(b, e->pd_n, b->precision == CR_CHOSEN_C64R);
+        // batched rays grouped by Pade order, then work; a tile holds
+        // floor(32/G) rays of G lanes each, G = the largest np in the tile
+        std::vector<int> bord;
+        for (int rid : order)
+            if (!is_col[(size_t)rid]) bord.push_back(rid);
+        // A tile marches in lockstep for its deepest ray's rows and its
+        // longest ray's steps, so its rays should agree in both: within a
+        // lane count G, rays are sorted by steps, and runs of 16 tiles'
+        // worth of rays by depth.
+        auto lanes_of = [&](int rid) { return (b->rays[rid].np + crk::kT - 1) / crk::kT; };
+        std::stable_sort(bord.begin(), bord.end(), [&](int x, int y) {
+            const int gx = lanes_of(x), gy = lanes_of(y);
+            if (gx != gy) return gx > gy;
+            return b->rays[x].nr > b->rays[y].nr;
+        });
+        for (size_t q = 0; q < bord.size();) {
+            const int G = lanes_of(bord[q]);
+            size_t gend = q;
+            while (gend < bord.size() && lanes_of(bord[gend]) == G) ++gend;
+            const size_t bucket = (size_t)16 * (kTile / G);
+            for (size_t k = q; k < gend; k += bucket)
+                std::stable_sort(bord.begin() + k, bord.begin() + std::min(gend, k + bucket),
+                                 [&](int x, int y) { return b->rays[x].nz > b->rays[y].nz; });
+            q = gend;
+        }
         e->rays.resize(b->n_rays);
         long long off = 0;
         size_t pos = 0;
-        while (pos < order.size()) {
+        while (pos < bord.size()) {
             // lanes per ray: each lane carries kT terms of the tile's largest np
-            const int G = (b->rays[order[pos]].np + crk::kT - 1) / crk::kT;
+            const int G = (b->rays[bord[pos]].np + crk::kT - 1) / crk::kT;
             const int R = kTile / G;
-            const size_t end = std::min(order.size(), pos + (size_t)R);
+            const size_t end = std::min(bord.size(), pos + (size_t)R);
             int rows = 0;
-            for (size_t q = pos; q < end; ++q) rows = std::max(rows, b->rays[order[q]].nz + 2);
+            for (size_t q = pos; q < end; ++q) rows = std::max(rows, b->rays[bord[q]].nz + 2);
             const int t = (int)e->tile_G.size();
             e->tile_G.push_back(G);
             e->tile_off.push_back(off);
@@ -898,41 +1058,66 @@ int cr_create(const cr_batch* b, cr_engine** out) {
             e->tile_ray.resize((size_t)(t + 1) * kTile, -1);
             for (size_t q = pos; q < end; ++q) {
                 const int slot = (int)(q - pos);
-                const int rid = order[q];
+                const int rid = bord[q];
                 for (int k = 0; k < G; ++k) e->tile_ray[(size_t)t * kTile + slot * G + k] = rid;
-                const cr_ray& r = b->rays[rid];
                 RayDev& d = e->rays[rid];
-                d.k0 = 2.0 * M_PI * r.freq / r.c0;
-                d.omega = 2.0 * M_PI * r.freq;
-                d.c0 = r.c0;
-                d.dz = r.dz;
-                d.dr = r.dr;
-                d.zmax = r.zmax;
-                d.lyrw_lambda = r.lyrw_lambda;
-                d.attnf = r.attnf;
-                d.rs = r.rs;
-                d.zs = r.zs;
-                d.zr = r.zr;
-                d.nz = r.nz;
-                d.nr = r.nr;
-                d.np = r.np;
-                d.ndr = r.ndr;
-                d.ndz = r.ndz;
-                d.nvr = r.nvr;
-                d.nvz = r.nvz;
-                d.env = r.env;
-                d.line_off = r.line_off;
-                d.grid_off = b->compute_grids ? r.grid_off : -1;
+                d = ray_dev(b->rays[rid], b->compute_grids);
                 d.col = off + slot;
-                d.ccol = -1;
                 d.crows = rows;
-                d.pad_ = 0;
-                e->point_updates += (double)r.nz * (double)r.nr;
+                e->point_updates += (double)b->rays[rid].nz * (double)b->rays[rid].nr;
             }
             off += (long long)rows * kTile;
             pos = end;
         }
         e->n_tiles = (int)e->tile_G.size();
+        e->term_capacity.assign((size_t)b->n_rays, 0);
+        for (int t = 0; t < e->n_tiles; ++t)
+            for (int l = 0; l < kTile; ++l) {
+                const int rid = e->tile_ray[(size_t)t * kTile + l];
+                if (rid >= 0) e->term_capacity[(size_t)rid] = e->tile_G[t] * crk::kT;
+            }
+        // column rays: grouped by Pade term count (the cluster size), deepest
+        // first; their ray columns are packed 32 to a tile after the batched ones
+        std::vector<int> cord;
+        for (int rid : order)
+            if (is_col[(size_t)rid]) cord.push_back(rid);
+        auto terms_of = [&](int rid) { return col_terms(e->pd_n, rid); };
+        const bool chosen = b->precision == CR_CHOSEN_C64R;
+        const std::vector<int> csize = column_clusters(b, e->pd_n, is_col, chosen);
+        std::stable_sort(cord.begin(), cord.end(), [&](int x, int y) {
+            const int tx = terms_of(x), ty = terms_of(y);
+            if (tx != ty) return tx > ty;
+            if (csize[(size_t)x] != csize[(size_t)y]) return csize[(size_t)x] > csize[(size_t)y];
+            return b->rays[x].nz > b->rays[y].nz;
+        });
+        for (size_t q = 0; q < cord.size(); q += kTile) {
+            const size_t end = std::min(cord.size(), q + (size_t)kTile);
+            int rows = 0;
+            for (size_t k = q; k < end; ++k) rows = std::max(rows, b->rays[cord[k]].nz + 2);
+            for (size_t k = q; k < end; ++k) {
+                const int rid = cord[k];
+                RayDev& d = e->rays[rid];
+                d = ray_dev(b->rays[rid], b->compute_grids);
+                d.col = off + (long long)(k - q);
+                d.crows = rows;
+                e->point_updates += (double)b->rays[rid].nz * (double)b->rays[rid].nr;
+            }
+            off += (long long)rows * kTile;
+        }
+        // one launch per run of equal term count and cluster size (rays are
+        // sorted by depth within a term count)
+        for (size_t q = 0; q < cord.size();) {
+            size_t end = q;
+            const int terms = terms_of(cord[q]);
+            const int nz_max = b->rays[cord[q]].nz;
+            const int cluster = csize[(size_t)cord[q]];
+            while (end < cord.size() && terms_of(cord[end]) == terms && csize[(size_t)cord[end]] == cluster) ++end;
+            e->col_groups.push_back({cluster, terms, nz_max, (int)q, (int)(end - q), nullptr, nullptr});
+            q = end;
+        }
+        for (const auto& g : e->col_groups)
+            for (int k = g.begin; k < g.begin + g.count; ++k) e->term_capacity[(size_t)cord[k]] = g.terms;
+        e->col_ray = cord;
         e->col_elems = off;
         e->fac_elems = 0;
     } else {
@@ -1029,6 +1214,24 @@ int cr_create(const cr_batch* b, cr_engine** out) {
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tile_off, e->tile_off.size());
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_pfc, e->pfc.size());
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_pfcinf, e->pfcinf.size());
+        if (ce == cudaSuccess && !e->col_ray.empty()) ce = dev_alloc(e, &e->d_col_ray, e->col_ray.size());
+        if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->ev_fork, cudaEventDisableTiming);
+        {
+            // one stream per run of equal lanes per ray (the first is the engine's)
+            int runs = 0;
+            for (int t = 0; t < e->n_tiles; ++t) runs += (t == 0 || e->tile_G[t] != e->tile_G[t - 1]);
+            e->sum_streams.assign((size_t)std::max(runs, 1), nullptr);
+            e->sum_done.assign(e->sum_streams.size(), nullptr);
+            e->sum_streams[0] = e->stream;
+            for (size_t i = 1; i < e->sum_streams.size(); ++i)
+                if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&e->sum_streams[i], cudaStreamNonBlocking);
+            for (auto& ev : e->sum_done)
+                if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        }
+        for (auto& g : e->col_groups) {
+            if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking);
+            if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming);
+        }
     }
     if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tll, (size_t)e->line_len);
     if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_cpl, (size_t)e->line_len);
@@ -1055,6 +1258,7 @@ int cr_create(const cr_batch* b, cr_engine** out) {
     e->st.tile_rays = kTile;
     e->st.n_tiles = e->n_tiles;
     e->st.device_bytes = e->device_bytes;
+    e->st.column_rays = (int)e->col_ray.size();
     *out = e;
     return CR_OK;
 }
@@ -1063,6 +1267,9 @@ int cr_set_pade(cr_engine* e, int ray, int which, int n, const double* pd1, cons
     if (!e) return CR_EINVAL;
     if (ray < 0 || ray >= e->n_rays || which < 0 || which >= kSets || n < 1 || n > CR_MAX_NP || !pd1 || !pd2)
         return e->fail(CR_EINVAL, "cr_set_pade: invalid arguments");
+    if (e->sum_mode && n > e->term_capacity[(size_t)ray])
+        return e->fail(CR_EINVAL, "cr_set_pade: %d terms exceed the %d this ray's march was laid out for "
+                                  "(create the engine with np >= %d)", n, e->term_capacity[(size_t)ray], n);
     double2* p1 = e->pd1.data() + ((size_t)ray * kSets + which) * CR_MAX_NP;
     double2* p2 = e->pd2.data() + ((size_t)ray * kSets + which) * CR_MAX_NP;
     for (int j = 0; j < CR_MAX_NP; ++j) {
@@ -1070,6 +1277,7 @@ int cr_set_pade(cr_engine* e, int ray, int which, int n, const double* pd1, cons
         p2[j] = j < n ? make_double2(pd2[2 * j], pd2[2 * j + 1]) : make_double2(0.0, 0.0);
     }
     e->pd_n[(size_t)ray * kSets + which] = n;
+    if (e->sum_mode) partial_fractions(e, ray, which);
     e->uploaded = false;
     return CR_OK;
 }
@@ -1095,6 +1303,7 @@ int cr_upload(cr_engine* e) {
         cp(e->d_tile_loff, e->tile_loff.data(), e->tile_loff.size() * sizeof(long long));
         cp(e->d_pfc, e->pfc.data(), e->pfc.size() * sizeof(double2));
         cp(e->d_pfcinf, e->pfcinf.data(), e->pfcinf.size() * sizeof(double2));
+        cp(e->d_col_ray, e->col_ray.data(), e->col_ray.size() * sizeof(int));
     }
     if (ce == cudaSuccess) ce = cudaEventRecord(e->ev[1], e->stream);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
@@ -1171,12 +1380,54 @@ int cr_march(cr_engine* e) {
         sa.cpg = e->d_cpg;
         sa.flags = e->d_flags;
         sa.compute_grids = e->compute_grids;
+        crk::ColArgs ca;
+        ca.rays = e->d_rays;
+        ca.col_ray = e->d_col_ray;
+        ca.envs = e->d_envs;
+        ca.pool = e->d_pool;
+        ca.pd2 = e->d_pd2;
+        ca.pd_n = e->d_pd_n;
+        ca.pfc = e->d_pfc;
+        ca.pfcinf = e->d_pfcinf;
+        ca.f1 = e->d_f1;
+        ca.f2 = e->d_f2;
+        ca.f3 = e->d_f3;
+        ca.ksq = e->d_ksq;
+        ca.tll = e->d_tll;
+        ca.cpl = e->d_cpl;
+        ca.tlg = e->d_tlg;
+        ca.cpg = e->d_cpg;
+        ca.flags = e->d_flags;
+        ca.compute_grids = e->compute_grids;
+        const int chosen = e->precision == CR_CHOSEN_C64R;
         ce = cudaEventRecord(e->ev[0], e->stream);
-        sa.tile_begin = 0;
         int nl = 0;
+        // column groups first, each on its own stream (they hold the longest
+        // marches), then the batched tiles on the engine's stream
+        if (ce == cudaSuccess) ce = cudaEventRecord(e->ev_fork, e->stream);
+        for (size_t i = 1; i < e->sum_streams.size(); ++i)
+            if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->sum_streams[i], e->ev_fork, 0);
+        for (auto& g : e->col_groups) {
+            if (ce == cudaSuccess) ce = cudaStreamWaitEvent(g.stream, e->ev_fork, 0);
+            crk::ColArgs ga = ca;
+            ga.col_ray = e->d_col_ray + g.begin;
+            if (ce == cudaSuccess) ce = crk::launch_march_col(ga, g.count, g.cluster, g.terms, g.nz_max, chosen, g.stream);
+            if (ce == cudaSuccess) ce = cudaEventRecord(g.done, g.stream);
+            ++nl;
+        }
+        sa.tile_begin = 0;
+        int nb = 0;
         if (ce == cudaSuccess)
-            ce = crk::launch_march_sum(sa, e->tile_G.data(), e->n_tiles, e->precision == CR_CHOSEN_C64R, e->stream, &nl);
-        e->st.kernel_launches = nl;
+            ce = crk::launch_march_sum(sa, e->tile_G.data(), e->n_tiles, chosen, e->sum_streams.data(),
+                                       (int)e->sum_streams.size(), &nb);
+        for (size_t i = 1; i < e->sum_streams.size(); ++i) {
+            if (ce == cudaSuccess) ce = cudaEventRecord(e->sum_done[i], e->sum_streams[i]);
+            if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->stream, e->sum_done[i], 0);
+        }
+        for (auto& g : e->col_groups)
+            if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->stream, g.done, 0);
+        e->st.kernel_launches = nl + nb;
+        e->st.column_launches = nl;
     } else if (ce == cudaSuccess) {
         ce = cudaEventRecord(e->ev[0], e->stream);
         if (ce == cudaSuccess) {

@@ -735,8 +735,8 @@ static cudaError_t launch_p(const SumArgs& a, int p, int count, cudaStream_t st)
     }
 }
 
-cudaError_t launch_march_sum(const SumArgs& a0, const int* tile_P, int n_tiles, int chosen, cudaStream_t st,
-                             int* launches) {
+cudaError_t launch_march_sum(const SumArgs& a0, const int* tile_P, int n_tiles, int chosen,
+                             const cudaStream_t* streams, int n_streams, int* launches) {
     // tiles are ordered by lanes per ray; one launch per run of equal P
     int begin = 0;
     *launches = 0;
@@ -745,6 +745,7 @@ cudaError_t launch_march_sum(const SumArgs& a0, const int* tile_P, int n_tiles, 
         while (end < n_tiles && tile_P[end] == tile_P[begin]) ++end;
         SumArgs a = a0;
         a.tile_begin = begin;
+        const cudaStream_t st = streams[*launches % n_streams];
         const cudaError_t ce = chosen ? launch_p<float>(a, tile_P[begin], end - begin, st)
                                       : launch_p<double>(a, tile_P[begin], end - begin, st);
         if (ce != cudaSuccess) return ce;

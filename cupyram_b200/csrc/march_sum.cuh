@@ -48,9 +48,10 @@ struct SumArgs {
 // for G and the factors are then read as float2).
 // Largest lanes-per-ray value the kernels are instantiated for (np <= 10).
 constexpr int kMaxP = (10 + kT - 1) / kT;
-// tile_P: host copy of tile_G.  One launch per run of equal P; the number of
+// tile_P: host copy of tile_G.  One launch per run of equal P: run i goes
+// on streams[i % n_streams] (independent runs overlap); the number of
 // launches is returned in *launches.
-cudaError_t launch_march_sum(const SumArgs& a, const int* tile_P, int n_tiles, int chosen, cudaStream_t st,
-                             int* launches);
+cudaError_t launch_march_sum(const SumArgs& a, const int* tile_P, int n_tiles, int chosen,
+                             const cudaStream_t* streams, int n_streams, int* launches);
 
 }  // namespace crk

@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define CR_ABI_VERSION 1
+#define CR_ABI_VERSION 2
 /* Largest number of Pade terms a ray may use. */
 #define CR_MAX_NP 10
 
@@ -123,6 +123,8 @@ typedef struct cr_stats {
     int32_t tile_rays;        /* rays per tile in the device layout             */
     int32_t n_tiles;
     int64_t device_bytes;     /* device memory held by the engine               */
+    int32_t column_rays;      /* rays marched by the column-parallel kernel      */
+    int32_t column_launches;  /* cluster launches of the last cr_march           */
 } cr_stats;
 
 typedef struct cr_engine cr_engine;

@@ -22,8 +22,10 @@ def _errs(ref, tl):
     return d.max(), np.sqrt(np.mean(d * d))
 
 
+@pytest.mark.parametrize("march", ["batched", "column"])
 @pytest.mark.parametrize("name", CASES)
-def test_chosen_vs_plain_golden(cuda_device, name):
+def test_chosen_vs_plain_golden(cuda_device, monkeypatch, name, march):
+    monkeypatch.setenv("CUPYRAM_B200_COL", "0" if march == "batched" else "1")
     args, kw, _ = load_case(name)
     envs, p, zs, zr, pr = B.prepare(*args, dict(kw))
     b = B.build_batch(envs, p, zs, zr, pr, True)

@@ -29,12 +29,20 @@ def _batch(name, grids=True):
     return B.build_batch(envs, p, zs, zr, pr, grids), fx
 
 
+@pytest.mark.parametrize("march", ["batched", "column"])
 @pytest.mark.parametrize("name", CASES)
-def test_engine_vs_oracle(cuda_device, name):
+def test_engine_vs_oracle(cuda_device, monkeypatch, name, march):
+    """Both march kernels: batched tiles (CUPYRAM_B200_COL=0) and one cluster per ray (=1)."""
+    monkeypatch.setenv("CUPYRAM_B200_COL", "0" if march == "batched" else "1")
     b, _ = _batch(name)
     with Engine(b) as eng:
         out = eng.run()
-        assert eng.stats()["rays_failed"] == 0
+        st = eng.stats()
+        assert st["rays_failed"] == 0
+        if march == "column":
+            assert st["column_rays"] == b.n_rays and st["column_launches"] >= 1
+        else:
+            assert st["column_rays"] == 0
     ref = oracle.run(b, "plain")
     n = b.line_len
     d = np.abs(out["tll"][:n] - ref["tll"][:n])
@@ -61,6 +69,42 @@ def test_cupyram_vs_reference(cuda_device, name):
     assert grid.shape == fx["tl_grid"].shape
     dg = np.abs(grid - fx["tl_grid"])
     assert np.percentile(dg, 99) <= TOL_REF and dg.max() <= 0.05
+
+
+def test_pekeris_full_size_column_march(cuda_device):
+    """The single-ray Pekeris configuration (nz 2399, 4999 steps, np 8, TL grid): the
+    default policy marches it on one cluster; TL line and grid against the oracle."""
+    from cupyram_b200 import workloads
+    b = workloads.build(*workloads.pekeris(), compute_grids=True)
+    with Engine(b) as eng:
+        out = eng.run()
+        st = eng.stats()
+    assert st["column_rays"] == 1 and st["rays_failed"] == 0
+    ref = oracle.run(b, "plain")
+    n = b.line_len
+    assert np.abs(out["tll"][:n] - ref["tll"][:n]).max() < TOL_ORACLE
+    g = np.abs(out["tlg"][:b.grid_len] - ref["tlg"][:b.grid_len])
+    assert np.percentile(g, 99.9) < TOL_ORACLE
+
+
+@pytest.mark.parametrize("rays", [3, 5])
+def test_column_march_deep_columns_vs_oracle(cuda_device, monkeypatch, rays):
+    """Deep Munk columns (nz 5350-5800) on the column kernel: clusters of up to
+    16 CTAs whose slices differ in length, against the oracle and against the
+    batched kernel on the same rays."""
+    from cupyram_b200 import workloads
+    b = workloads.build(*workloads.munk_batch(rays, seed=5, rmax=1500.0), compute_grids=False)
+    monkeypatch.setenv("CUPYRAM_B200_COL", "1")
+    with Engine(b) as eng:
+        out = eng.run()
+        assert eng.stats()["column_rays"] == rays
+    monkeypatch.setenv("CUPYRAM_B200_COL", "0")
+    with Engine(b) as eng:
+        bat = eng.run()
+    ref = oracle.run(b, "plain")
+    n = b.line_len
+    assert np.abs(out["tll"][:n] - ref["tll"][:n]).max() < TOL_ORACLE
+    assert np.abs(out["tll"][:n] - bat["tll"][:n]).max() < TOL_ORACLE
 
 
 def test_ram_v15_vs_fortran(cuda_device):
