@@ -74,6 +74,8 @@ _SIGS = {
     "cr_global_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
     "cr_destroy": (None, [ctypes.c_void_p]),
     "cr_march_static": (ctypes.c_int, [ctypes.POINTER(CrBatch), ctypes.POINTER(CrOutputs), ctypes.c_void_p]),
+    "cr_cell_tl": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                  ctypes.c_void_p]),
 }
 
 STATIC_SCRATCH_BYTES = 32 * 1024 * 1024  # CR_STATIC_SCRATCH_BYTES

@@ -246,10 +246,17 @@ def derive_params(envs, freqs, per_ray, kwargs, np_default=8, dzf=0.1, ndr_defau
         rmax = np.full(n_calc, float(kwargs.get("rmax", rmax_default)))
     if np.any(dr <= 0) or np.any(dz <= 0):
         raise ValueError("dr and dz must be positive")
-    ndr = int(kwargs.get("ndr", ndr_default))
-    ndz = int(kwargs.get("ndz", ndz_default))
-    if ndr < 1 or ndz < 1:
-        raise ValueError("ndr and ndz must be >= 1")
+    if per_ray and (np.ndim(kwargs.get("ndr", 1)) or np.ndim(kwargs.get("ndz", 1))):
+        # per-ray output decimation (an extension of per_ray mode)
+        ndr = _per_calc(kwargs.get("ndr", ndr_default), n_env, "ndr", np.int64)
+        ndz = _per_calc(kwargs.get("ndz", ndz_default), n_env, "ndz", np.int64)
+        if np.any(ndr < 1) or np.any(ndz < 1):
+            raise ValueError("ndr and ndz must be >= 1")
+    else:
+        ndr = int(kwargs.get("ndr", ndr_default))
+        ndz = int(kwargs.get("ndz", ndz_default))
+        if ndr < 1 or ndz < 1:
+            raise ValueError("ndr and ndz must be >= 1")
     ns = int(kwargs.get("ns", ns_default))
     if ns not in (0, 1, 2):
         raise ValueError("ns must be 0, 1 or 2")
@@ -326,8 +333,8 @@ def build_batch(envs, p: Params, zs, zr, per_ray, compute_grids):
         r["nr"] = nr[b]
         r["np"] = p.np_pade[b]
         r["ns"] = p.ns
-        r["ndr"] = p.ndr
-        r["ndz"] = p.ndz
+        r["ndr"] = p.ndr[b] if np.ndim(p.ndr) else p.ndr
+        r["ndz"] = p.ndz[b] if np.ndim(p.ndz) else p.ndz
         r["nvr"] = nvr[b]
         r["nvz"] = nvz[b]
         r["env"] = e
@@ -341,8 +348,10 @@ def build_batch(envs, p: Params, zs, zr, per_ray, compute_grids):
     for b in range(n_calc):
         if int(np.floor(zs[b // n_freq] / p.dz[b])) + 1 > nz[b]:
             raise ValueError(f"Ray {b}: source depth below the computational grid")
-    vr = [np.arange(1, nvr[b] + 1) * p.dr[b] * p.ndr for b in range(n_calc)]
-    vz = [np.arange(1, nvz[b] + 1) * p.dz[b] * p.ndz for b in range(n_calc)]
+    ndr_b = np.broadcast_to(p.ndr, (n_calc,))
+    ndz_b = np.broadcast_to(p.ndz, (n_calc,))
+    vr = [np.arange(1, nvr[b] + 1) * p.dr[b] * ndr_b[b] for b in range(n_calc)]
+    vz = [np.arange(1, nvz[b] + 1) * p.dz[b] * ndz_b[b] for b in range(n_calc)]
     return Batch(rays, env_arr, pool, line_off, grid_off, bool(compute_grids), n_env, n_freq,
                  per_ray, nz, nvr, nvz, zmax, vr, vz)
 

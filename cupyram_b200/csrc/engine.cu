@@ -1481,6 +1481,61 @@ int cr_download(cr_engine* e, const cr_outputs* out) {
     return CR_OK;
 }
 
+namespace {
+
+// TL of cells of sz x sr grid outputs (rows j sz .. j sz + sz - 1, ranges
+// c sr .. c sr + sr - 1 of the ray's TL grid): -10 log10 of the mean of
+// |cp|^2 / r over the cell, r = (t + 1) ndr dr.  NaN where the ray's grid is
+// smaller than the cells asked for.
+__global__ void cell_tl_kernel(const RayDev* __restrict__ rays, int n_rays, const double2* __restrict__ cpg, int sz,
+                               int sr, int ncz, int ncr, float* __restrict__ out) {
+    const long long total = (long long)n_rays * ncz * ncr;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int ray = (int)(i / ((long long)ncz * ncr));
+        const int rem = (int)(i % ((long long)ncz * ncr));
+        const int j = rem / ncr, c = rem % ncr;
+        const RayDev& ry = rays[ray];
+        if (ry.grid_off < 0 || (j + 1) * sz > ry.nvz || (c + 1) * sr > ry.nvr) {
+            out[i] = __int_as_float(0x7fc00000);
+            continue;
+        }
+        double acc = 0.0;
+        for (int a = 0; a < sz; ++a) {
+            const double2* row = cpg + ry.grid_off + (long long)(j * sz + a) * ry.nvr;
+            for (int b = 0; b < sr; ++b) {
+                const int t = c * sr + b;
+                const double2 p = row[t];
+                acc += (p.x * p.x + p.y * p.y) / ((double)((t + 1) * ry.ndr) * ry.dr);
+            }
+        }
+        out[i] = (float)(-10.0 * log10(acc / (double)(sz * sr)));
+    }
+}
+
+}  // namespace
+
+int cr_cell_tl(cr_engine* e, int sz, int sr, int ncz, int ncr, float* tl_cells) {
+    if (!e) return CR_EINVAL;
+    if (sz < 1 || sr < 1 || ncz < 1 || ncr < 1 || !tl_cells) return e->fail(CR_EINVAL, "cr_cell_tl: invalid arguments");
+    if (!e->compute_grids) return e->fail(CR_EINVAL, "cr_cell_tl: the batch computes no TL grid");
+    if (!e->marched) return e->fail(CR_ESTATE, "cr_cell_tl: nothing marched yet");
+    const size_t n = (size_t)e->n_rays * ncz * ncr;
+    float* d_out = nullptr;
+    cudaError_t ce = cudaSetDevice(e->device);
+    if (ce == cudaSuccess) ce = cudaMallocAsync((void**)&d_out, n * sizeof(float), e->stream);
+    if (ce == cudaSuccess) {
+        const long long blocks = std::min<long long>(((long long)n + 255) / 256, 65535);
+        cell_tl_kernel<<<(unsigned)blocks, 256, 0, e->stream>>>(e->d_rays, e->n_rays, e->d_cpg, sz, sr, ncz, ncr, d_out);
+        ce = cudaGetLastError();
+    }
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(tl_cells, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, e->stream);
+    if (d_out) cudaFreeAsync(d_out, e->stream);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) return e->cuda_fail(ce, "cr_cell_tl");
+    return CR_OK;
+}
+
 int cr_run(cr_engine* e, const cr_outputs* out) {
     int rc = cr_upload(e);
     if (rc) return rc;

@@ -1,0 +1,304 @@
+// mlp.cu - BF16 tensor-core kernels of the learned surrogate (training and
+// inference of its MLP ensemble), FP32 accumulation.
+//
+// Every contraction of the MLP is one kernel, C = A B^T with both operands
+// K-contiguous ("TN"):
+//     forward        Y[B,N]  = X[B,K]  W[N,K]^T            (+ bias, ReLU)
+//     input grad     dX[B,K] = dY[B,N] (W^T)[K,N]^T         (x ReLU mask)
+//     weight grad    dW[N,K] = (dY^T)[N,B] (X^T)[K,B]^T
+// with transposed BF16 copies of W, dY and X made by a tiled transpose.  The
+// tile loop stages 128 x 32 tiles of A and B in shared memory with cp.async
+// (two stages, XOR-swizzled 16-byte chunks so that ldmatrix reads are
+// conflict-free), and each of 8 warps runs mma.sync m16n8k16 (bf16 x bf16 ->
+// f32) on a 64 x 32 piece of the 128 x 128 block.  Shapes must be multiples of
+// the tile (M, N of 128, K of 32); the host wrappers check that and the
+// 16-byte alignment of every row.
+//
+// Plus the small kernels of a training step: column sums (bias gradients),
+// the masked mean-squared-error gradient, Adam, and BF16 conversion.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/cupyram_b200_mlp.h"
+
+namespace {
+
+constexpr int BM = 128, BN = 128, BK = 32;
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void ldsm_x4(uint32_t& r0, uint32_t& r1, uint32_t& r2, uint32_t& r3, const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r0), "=r"(r1), "=r"(r2), "=r"(r3)
+                 : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void mma_bf16(float* c, const uint32_t* a, uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Shared tile: 128 rows x 32 bf16 (four 16-byte chunks per row); chunk c of
+// row r is stored at chunk c ^ ((r >> 1) & 3).
+__device__ __forceinline__ int swz(int row, int chunk) { return row * BK + ((chunk ^ ((row >> 1) & 3)) << 3); }
+
+struct EpiArgs {
+    void* out;
+    int ldo;
+    const float* bias;
+    const __nv_bfloat16* mask;
+    int ldm;
+};
+
+template <int EPI>
+__device__ __forceinline__ void store2(const EpiArgs& e, int row, int col, float v0, float v1) {
+    if (EPI == CR_MLP_EPI_BIAS_RELU_BF16) {
+        v0 = fmaxf(v0 + e.bias[col], 0.f);
+        v1 = fmaxf(v1 + e.bias[col + 1], 0.f);
+        *reinterpret_cast<__nv_bfloat162*>((__nv_bfloat16*)e.out + (size_t)row * e.ldo + col) =
+            __floats2bfloat162_rn(v0, v1);
+    } else if (EPI == CR_MLP_EPI_BIAS_F32) {
+        *reinterpret_cast<float2*>((float*)e.out + (size_t)row * e.ldo + col) =
+            make_float2(v0 + e.bias[col], v1 + e.bias[col + 1]);
+    } else if (EPI == CR_MLP_EPI_F32) {
+        *reinterpret_cast<float2*>((float*)e.out + (size_t)row * e.ldo + col) = make_float2(v0, v1);
+    } else {  // CR_MLP_EPI_RELU_MASK_BF16: gradient through the ReLU whose output is `mask`
+        const __nv_bfloat162 m = *reinterpret_cast<const __nv_bfloat162*>(e.mask + (size_t)row * e.ldm + col);
+        v0 = __bfloat162float(m.x) > 0.f ? v0 : 0.f;
+        v1 = __bfloat162float(m.y) > 0.f ? v1 : 0.f;
+        *reinterpret_cast<__nv_bfloat162*>((__nv_bfloat16*)e.out + (size_t)row * e.ldo + col) =
+            __floats2bfloat162_rn(v0, v1);
+    }
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(kThreads) gemm_tn(const __nv_bfloat16* __restrict__ A,
+                                                     const __nv_bfloat16* __restrict__ B, int K, int lda, int ldb,
+                                                     EpiArgs e) {
+    __shared__ __align__(128) __nv_bfloat16 sA[2][BM * BK];
+    __shared__ __align__(128) __nv_bfloat16 sB[2][BN * BK];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = warp & 1, wn = warp >> 1;  // 2 x 4 warps: 64 rows x 32 columns each
+    const int bm = blockIdx.y * BM, bn = blockIdx.x * BN;
+    const __nv_bfloat16* Ab = A + (size_t)bm * lda;
+    const __nv_bfloat16* Bb = B + (size_t)bn * ldb;
+
+    auto load = [&](int stage, int k0) {
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const int c = tid + i * kThreads;  // 512 chunks of 16 bytes per tile
+            const int row = c >> 2, ch = c & 3;
+            cp_async16(&sA[stage][swz(row, ch)], Ab + (size_t)row * lda + k0 + ch * 8);
+            cp_async16(&sB[stage][swz(row, ch)], Bb + (size_t)row * ldb + k0 + ch * 8);
+        }
+        cp_commit();
+    };
+
+    float acc[4][4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) acc[i][j][q] = 0.f;
+
+    const int nk = K / BK;
+    load(0, 0);
+    for (int kt = 0; kt < nk; ++kt) {
+        const int st = kt & 1;
+        if (kt + 1 < nk) {
+            load(st ^ 1, (kt + 1) * BK);
+            cp_wait<1>();
+        } else {
+            cp_wait<0>();
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < 2; ++ks) {
+            uint32_t a[4][4], b[4][2];
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi) {
+                const int row = wm * 64 + mi * 16 + (lane & 15);
+                ldsm_x4(a[mi][0], a[mi][1], a[mi][2], a[mi][3], &sA[st][swz(row, ks * 2 + (lane >> 4))]);
+            }
+#pragma unroll
+            for (int nj = 0; nj < 2; ++nj) {
+                const int row = wn * 32 + nj * 16 + (lane & 7) + ((lane >> 4) << 3);
+                ldsm_x4(b[2 * nj][0], b[2 * nj][1], b[2 * nj + 1][0], b[2 * nj + 1][1],
+                        &sB[st][swz(row, ks * 2 + ((lane >> 3) & 1))]);
+            }
+#pragma unroll
+            for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) mma_bf16(acc[mi][ni], a[mi], b[ni][0], b[ni][1]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int mi = 0; mi < 4; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+            const int row = bm + wm * 64 + mi * 16 + (lane >> 2);
+            const int col = bn + wn * 32 + ni * 8 + (lane & 3) * 2;
+            store2<EPI>(e, row, col, acc[mi][ni][0], acc[mi][ni][1]);
+            store2<EPI>(e, row + 8, col, acc[mi][ni][2], acc[mi][ni][3]);
+        }
+}
+
+// dst[c][r] = src[r][c] for a rows x cols BF16 matrix (32 x 32 tiles).
+__global__ void transpose_bf16(const __nv_bfloat16* __restrict__ src, int lds, __nv_bfloat16* __restrict__ dst,
+                               int ldd, int rows, int cols) {
+    __shared__ __nv_bfloat16 t[32][33];
+    const int r0 = blockIdx.y * 32, c0 = blockIdx.x * 32;
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int r = r0 + i, c = c0 + threadIdx.x;
+        if (r < rows && c < cols) t[i][threadIdx.x] = src[(size_t)r * lds + c];
+    }
+    __syncthreads();
+    for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+        const int c = c0 + i, r = r0 + threadIdx.x;
+        if (r < rows && c < cols) dst[(size_t)c * ldd + r] = t[threadIdx.x][i];
+    }
+}
+
+// out[c] = sum_r src[r][c] (bias gradients), one thread per column.
+__global__ void col_sum_bf16(const __nv_bfloat16* __restrict__ src, int ld, int rows, int cols, float* __restrict__ out) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    float s = 0.f;
+    for (int r = 0; r < rows; ++r) s += __bfloat162float(src[(size_t)r * ld + c]);
+    out[c] = s;
+}
+
+// Masked mean squared error: grad = 2 (pred - y) / n_valid where valid,
+// and the sum of squared errors accumulated into *sse.
+__global__ void mse_grad(const float* __restrict__ pred, const __nv_bfloat16* __restrict__ y,
+                         const unsigned char* __restrict__ valid, long long n, float inv_count,
+                         __nv_bfloat16* __restrict__ grad, double* __restrict__ sse) {
+    __shared__ double red[256];
+    double acc = 0.0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        float g = 0.f;
+        if (valid[i]) {
+            const float d = pred[i] - __bfloat162float(y[i]);
+            g = 2.f * d * inv_count;
+            acc += (double)d * d;
+        }
+        grad[i] = __float2bfloat16_rn(g);
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) atomicAdd(sse, red[0]);
+}
+
+// Adam on FP32 master parameters; writes the BF16 copy used by the GEMMs.
+__global__ void adam_step(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                          float* __restrict__ v, __nv_bfloat16* __restrict__ pb, long long n, float lr, float b1,
+                          float b2, float eps, float c1, float c2, float wd) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float gi = g[i] + wd * p[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        const float pi = p[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+        p[i] = pi;
+        if (pb) pb[i] = __float2bfloat16_rn(pi);
+    }
+}
+
+__global__ void to_bf16(const float* __restrict__ src, __nv_bfloat16* __restrict__ dst, long long n) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] = __float2bfloat16_rn(src[i]);
+}
+
+int grid_for(long long n) {
+    long long b = (n + 255) / 256;
+    return (int)(b < 4096 ? (b < 1 ? 1 : b) : 4096);
+}
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
+
+}  // namespace
+
+extern "C" {
+
+int cr_mlp_gemm(int epi, const void* A, const void* B, int M, int N, int K, int lda, int ldb, void* out, int ldo,
+                const float* bias, const void* mask, int ldm, void* stream) {
+    if (M <= 0 || N <= 0 || K <= 0 || M % BM || N % BN || K % BK) return CR_MLP_EBADSHAPE;
+    if (lda < K || ldb < K || lda % 8 || ldb % 8 || ldo < N || ldo % 2 || !aligned16(A) || !aligned16(B) || !out)
+        return CR_MLP_EBADSHAPE;
+    if ((epi == CR_MLP_EPI_BIAS_RELU_BF16 || epi == CR_MLP_EPI_BIAS_F32) && !bias) return CR_MLP_EBADSHAPE;
+    if (epi == CR_MLP_EPI_RELU_MASK_BF16 && (!mask || ldm < N || ldm % 2)) return CR_MLP_EBADSHAPE;
+    EpiArgs e{out, ldo, bias, (const __nv_bfloat16*)mask, ldm};
+    const dim3 grid(N / BN, M / BM);
+    cudaStream_t st = (cudaStream_t)stream;
+    auto a = (const __nv_bfloat16*)A;
+    auto b = (const __nv_bfloat16*)B;
+    switch (epi) {
+        case CR_MLP_EPI_BIAS_RELU_BF16: gemm_tn<CR_MLP_EPI_BIAS_RELU_BF16><<<grid, kThreads, 0, st>>>(a, b, K, lda, ldb, e); break;
+        case CR_MLP_EPI_BIAS_F32: gemm_tn<CR_MLP_EPI_BIAS_F32><<<grid, kThreads, 0, st>>>(a, b, K, lda, ldb, e); break;
+        case CR_MLP_EPI_F32: gemm_tn<CR_MLP_EPI_F32><<<grid, kThreads, 0, st>>>(a, b, K, lda, ldb, e); break;
+        case CR_MLP_EPI_RELU_MASK_BF16: gemm_tn<CR_MLP_EPI_RELU_MASK_BF16><<<grid, kThreads, 0, st>>>(a, b, K, lda, ldb, e); break;
+        default: return CR_MLP_EBADSHAPE;
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : CR_MLP_ECUDA;
+}
+
+int cr_mlp_transpose(const void* src, int lds, void* dst, int ldd, int rows, int cols, void* stream) {
+    if (rows <= 0 || cols <= 0 || lds < cols || ldd < rows) return CR_MLP_EBADSHAPE;
+    const dim3 grid((cols + 31) / 32, (rows + 31) / 32), block(32, 8);
+    transpose_bf16<<<grid, block, 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)src, lds, (__nv_bfloat16*)dst, ldd,
+                                                              rows, cols);
+    return cudaGetLastError() == cudaSuccess ? 0 : CR_MLP_ECUDA;
+}
+
+int cr_mlp_col_sum(const void* src, int ld, int rows, int cols, float* out, void* stream) {
+    if (rows <= 0 || cols <= 0 || ld < cols) return CR_MLP_EBADSHAPE;
+    col_sum_bf16<<<(cols + 255) / 256, 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)src, ld, rows, cols, out);
+    return cudaGetLastError() == cudaSuccess ? 0 : CR_MLP_ECUDA;
+}
+
+int cr_mlp_mse_grad(const float* pred, const void* target, const unsigned char* valid, long long n, float inv_count,
+                    void* grad, double* sse, void* stream) {
+    if (n <= 0) return CR_MLP_EBADSHAPE;
+    mse_grad<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(pred, (const __nv_bfloat16*)target, valid, n, inv_count,
+                                                            (__nv_bfloat16*)grad, sse);
+    return cudaGetLastError() == cudaSuccess ? 0 : CR_MLP_ECUDA;
+}
+
+int cr_mlp_adam(float* p, const float* g, float* m, float* v, void* p_bf16, long long n, float lr, float beta1,
+                float beta2, float eps, int step, float weight_decay, void* stream) {
+    if (n <= 0 || step < 1) return CR_MLP_EBADSHAPE;
+    const float c1 = 1.f / (1.f - powf(beta1, (float)step));
+    const float c2 = 1.f / (1.f - powf(beta2, (float)step));
+    adam_step<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(p, g, m, v, (__nv_bfloat16*)p_bf16, n, lr, beta1, beta2,
+                                                             eps, c1, c2, weight_decay);
+    return cudaGetLastError() == cudaSuccess ? 0 : CR_MLP_ECUDA;
+}
+
+int cr_mlp_to_bf16(const float* src, void* dst, long long n, void* stream) {
+    if (n <= 0) return CR_MLP_EBADSHAPE;
+    to_bf16<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(src, (__nv_bfloat16*)dst, n);
+    return cudaGetLastError() == cudaSuccess ? 0 : CR_MLP_ECUDA;
+}
+
+}  // extern "C"

@@ -84,6 +84,12 @@ class Engine:
         _lib.check(self.lib.cr_run(self.handle, ctypes.byref(o)), self.handle)
         return out
 
+    def cell_tl(self, sz, sr, ncz, ncr):
+        """[n_rays, ncz, ncr] float32 cell-averaged TL of the last march (cr_cell_tl)."""
+        out = np.empty((self.batch.n_rays, ncz, ncr), np.float32)
+        _lib.check(self.lib.cr_cell_tl(self.handle, sz, sr, ncz, ncr, out.ctypes.data), self.handle)
+        return out
+
     def set_pade(self, ray, which, pd1, pd2):
         p1 = np.ascontiguousarray(pd1, dtype=np.complex128)
         p2 = np.ascontiguousarray(pd2, dtype=np.complex128)

@@ -168,6 +168,15 @@ int cr_download(cr_engine* e, const cr_outputs* out);
 /* cr_upload + cr_march + cr_download: the whole CuPyRAM.run on the device. */
 int cr_run(cr_engine* e, const cr_outputs* out);
 
+/* Cell-averaged transmission loss, computed on the device from the last
+ * march's TL-grid outputs (no counterpart in the reference, whose grid can
+ * only be downloaded whole): cell (j, c) of a ray averages |p|^2 over the sz
+ * x sr grid outputs at rows j*sz .. j*sz+sz-1 and output ranges c*sr ..
+ * c*sr+sr-1, p^2 = |cp|^2 / r, and reports -10 log10 of the mean.
+ * tl_cells: host buffer of n_rays * ncz * ncr floats, [ray][j][c]; cells
+ * beyond a ray's grid are NaN.  Needs batch->compute_grids. */
+int cr_cell_tl(cr_engine* e, int sz, int sr, int ncz, int ncr, float* tl_cells);
+
 /* Override one ray's Pade set: which = 0 self-starter (1-X)^-2 factor,
  * 1 self-starter ip=2, 2 march, 3 march after rs.  n terms (<= CR_MAX_NP). */
 int cr_set_pade(cr_engine* e, int ray, int which, int n, const double* pd1, const double* pd2);
