@@ -27,6 +27,13 @@ Other configurations (--config):
   precision - the Munk batch at 16,384 rays with a coarse TL grid (ndr 20,
               ndz 100): TL errors of the chosen form against complex128 over
               the line and the grid, cells with TL < 100 dB
+  surrogate - the learned surrogate: 200,000 training marches of seeded
+              environments, an ensemble of 4 MLPs (4 layers, width 512, BF16,
+              FP32 accumulation) trained by the package's kernels, 65,536
+              served requests with fallback to the march above 1 dB of
+              ensemble spread, march reruns of a 1 % sample as the judge;
+              value = march grid-point updates the served requests stand for
+              per second of serving
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--form plain|chosen]
                        [--config munk|pekeris|wedge|precision]
@@ -60,7 +67,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--form", choices=["plain", "chosen"], default="plain")
-    ap.add_argument("--config", choices=["munk", "pekeris", "wedge", "precision"], default="munk")
+    ap.add_argument("--config", choices=["munk", "pekeris", "wedge", "precision", "surrogate"], default="munk")
+    ap.add_argument("--train", type=int, default=200_000, help="surrogate: training marches")
+    ap.add_argument("--infer", type=int, default=65_536, help="surrogate: served requests")
+    ap.add_argument("--epochs", type=int, default=12, help="surrogate: training epochs per member")
     ap.add_argument("--rays", type=int, default=0, help="rays per GPU (0: the configuration's own count)")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -286,8 +296,39 @@ def run_reference(a):
     return 0
 
 
+def run_surrogate(a):
+    """The learned surrogate's pipeline on one GPU (rank 0 only under torchrun)."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    import torch
+    torch.cuda.set_device(local)
+    from cupyram_b200 import surrogate as S
+    logs = []
+    with ClockSampler(local) as clk:
+        res = S.pipeline(n_train=a.train, n_infer=a.infer, epochs=a.epochs, seed=a.seed,
+                         log=lambda m: (logs.append(m), print(m, file=sys.stderr, flush=True)))
+    value = res["equivalent_updates_per_s"]
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": 1, "warmup": 0,
+            "ms_per_step": (res["net_seconds"] + res["fallback_march_seconds"]) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (network), complex128 (fallback march)",
+            "data": "synthetic (seeded environments; training fields computed by the march)",
+            "config": {"workload": f"learned surrogate: {a.train} training marches, {a.infer} served requests, "
+                                   "ensemble of 4 MLPs 128-512-512-512-8192, TL on 128 ranges x 64 depths "
+                                   "(0-20 km, 0-D0), fallback above 1 dB spread, 1 % judged by march reruns",
+                       "config": "surrogate", "seed": a.seed},
+            "e2e": {"value": res["equivalent_updates_per_s_wall"], "unit": UNIT,
+                    "h2d_bytes_per_step": int(a.infer * S.D_IN * 2),
+                    "d2h_bytes_per_step": int(a.infer * S.NZ_OUT * S.NR_OUT * 4)},
+            "surrogate": res, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
+    if a.config == "surrogate":
+        return run_surrogate(a)
     if a.impl == "reference":
         return run_reference(a)
     rank, world, local = dist_env()

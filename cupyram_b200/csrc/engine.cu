@@ -922,6 +922,25 @@ std::vector<int> column_clusters(const cr_batch* b, const std::vector<int>& pd_n
     return cl;
 }
 
+// Operator changes a ray's march will see: bathymetry-index moves (the
+// bottom's total depth excursion along the track over dz, capped at one per
+// step) plus profile updates.
+double operator_changes(const cr_batch* b, const cr_ray& r) {
+    const cr_env& v = b->envs[r.env];
+    const double* q = b->pool + v.off;
+    q += v.n_zss + v.n_rss + (long long)v.n_rss * v.n_zss + v.n_zsb + v.n_rsb + 3LL * v.n_rsb * v.n_zsb;
+    const double* rb = q;
+    const double* zb = q + v.n_bt;
+    const double rmax = r.dr * (r.nr + 1);
+    double excursion = 0.0;
+    for (int k = 0; k + 1 < v.n_bt && rb[k] < rmax; ++k) {
+        const double r1 = std::min(rb[k + 1], rmax);
+        const double frac = rb[k + 1] > rb[k] ? (r1 - rb[k]) / (rb[k + 1] - rb[k]) : 1.0;
+        excursion += std::fabs(zb[k + 1] - zb[k]) * frac;
+    }
+    return std::min(excursion / r.dz, (double)r.nr) + (double)(v.n_rss - 1) + (double)(v.n_rsb - 1);
+}
+
 // Rays marched by the column-parallel kernel instead of the batched one.
 // A ray's lockstep march in a batched tile takes about (nz + 2)(nr + 4)
 // row steps of one warp in sequence; when that alone exceeds the time the
@@ -942,7 +961,11 @@ std::vector<char> pick_column_rays(const cr_batch* b, const std::vector<int>& pd
     std::map<std::tuple<int, int, int>, bool> runs;
     for (int i = 0; i < b->n_rays; ++i) {
         const cr_ray& r = b->rays[i];
-        if (mode == 2 && (double)(r.nz + 2) * (r.nr + 4) * kRowStepSeconds <= tau) continue;
+        // every operator change (bathymetry index, profile update) costs the
+        // batched march about four more passes: back-substitution alone, two
+        // factorisation passes, elimination alone
+        const double steps = (double)(r.nr + 4) + 4.0 * operator_changes(b, r);
+        if (mode == 2 && (double)(r.nz + 2) * steps * kRowStepSeconds <= tau) continue;
         const int terms = col_terms(pd_n, i);
         const int cluster = crk::col_cluster_size(r.nz, terms, chosen);
         if (cluster == 0) continue;

@@ -30,8 +30,10 @@
 //
 // The Thomas factorisation of each term (1/den, al = -(a1 + p d1)/den and
 // w per row, top-down) is recomputed when the operator changes (profiles,
-// bathymetry index, Pade set): each CTA runs the recurrence from the first
-// changed row (or row 1) down to its slice's end, one lane per term.
+// bathymetry index, Pade set) by the same segment / scan / fold scheme: the
+// recurrence for w is linear in homogeneous coordinates (col_factor), so a
+// refactorisation costs about one step, however often a sloping bottom
+// moves the bathymetry index.
 //
 // Range logic, self-starter and outputs follow the batched march
 // (cupyram/cupyram.py:273-380 run, :1001-1063 selfs, updat.py:38-140,
@@ -134,7 +136,8 @@ __host__ __device__ inline size_t r16(size_t b) { return (b + 15) & ~(size_t)15;
 // value.  Every CTA of a cluster uses the same layout (that of the largest
 // slice), so that a remote CTA's tables sit at the same offsets.
 __host__ __device__ inline size_t col_bytes(int P, int terms, int nmax, size_t vb) {
-    return 2 * r16(2 * 16 * (size_t)terms) + r16(16 * (size_t)P) + 4 * r16(vb * (size_t)P * terms) +
+    return 2 * r16(2 * 16 * (size_t)terms) + r16(4 * 16 * (size_t)terms) + r16(16 * (size_t)P) +
+           4 * r16(vb * (size_t)P * terms) +
            r16(vb * terms) + r16(32 * (size_t)terms) + r16(16 * kColMaxTerms) + r16(16 * 3) +
            r16(4 * (size_t)(nmax + 2));
 }
@@ -151,6 +154,7 @@ struct ColSmem {
     V* wghost;      // [term] w of row R0 - 1
     double2* fwd;   // [term][2] elimination map of the slice (A, B), read by later CTAs
     double2* bwd;   // [term][2] back-substitution map of the slice, read by earlier CTAs
+    double2* fmat;  // [term][4] factorisation map of the slice (2 x 2), read by later CTAs
     double2* xh;    // [term][2] x of the halo rows R0 - 1 and R1 + 1
     double2* ck;    // [kColMaxTerms] residues of the active set
     double2* misc;  // [0] c_inf, [1] u of row R0 - 1, [2] u of row R1 + 1
@@ -170,6 +174,7 @@ __device__ ColSmem<R> carve(unsigned char* base, int P, int terms, int nmax) {
     // the tables other CTAs read come first
     s.fwd = (double2*)take(2 * 16 * (size_t)terms);
     s.bwd = (double2*)take(2 * 16 * (size_t)terms);
+    s.fmat = (double2*)take(4 * 16 * (size_t)terms);
     s.U = (double2*)take(16 * (size_t)P);
     s.Q = (V*)take(sizeof(V) * (size_t)P * terms);
     s.AL = (V*)take(sizeof(V) * (size_t)P * terms);
@@ -266,14 +271,60 @@ struct ColCtx {
     double cfact, a1, a2;
 };
 
-// Factors of rows lo..R1 of this warp's term, top-down, by lane 0 of the
-// warp.  The recurrence continues from the stored w of row lo - 1 when this
-// CTA holds it (lo - 1 >= R0 - 1), else it starts again at row 1.
+// 2 x 2 complex matrix [[a, b], [c, d]].
+struct M2 {
+    double2 a, b, c, d;
+};
+__device__ __forceinline__ double2 cadd(double2 x, double2 y) { return c2(x.x + y.x, x.y + y.y); }
+__device__ __forceinline__ M2 m2_mul(const M2& X, const M2& Y) {
+    return {cadd(cmul(X.a, Y.a), cmul(X.b, Y.c)), cadd(cmul(X.a, Y.b), cmul(X.b, Y.d)),
+            cadd(cmul(X.c, Y.a), cmul(X.d, Y.c)), cadd(cmul(X.c, Y.b), cmul(X.d, Y.d))};
+}
+// The maps act projectively (w = N / D), so a matrix may be rescaled at will:
+// keep its largest component near 1.
+__device__ __forceinline__ M2 m2_norm(M2 X) {
+    const double m = fmax(fmax(fmax(fabs(X.a.x), fabs(X.a.y)), fmax(fabs(X.b.x), fabs(X.b.y))),
+                          fmax(fmax(fabs(X.c.x), fabs(X.c.y)), fmax(fabs(X.d.x), fabs(X.d.y))));
+    if (m > 0.0 && isfinite(m)) {
+        const double s = 1.0 / m;
+        X.a = c2(X.a.x * s, X.a.y * s);
+        X.b = c2(X.b.x * s, X.b.y * s);
+        X.c = c2(X.c.x * s, X.c.y * s);
+        X.d = c2(X.d.x * s, X.d.y * s);
+    }
+    return X;
+}
+__device__ __forceinline__ M2 m2_eye() { return {c2(1.0, 0.0), c2(0.0, 0.0), c2(0.0, 0.0), c2(1.0, 0.0)}; }
+__device__ __forceinline__ M2 m2_shfl(const M2& X, int from) {
+    M2 r;
+    r.a = c2(__shfl_sync(0xffffffffu, X.a.x, from), __shfl_sync(0xffffffffu, X.a.y, from));
+    r.b = c2(__shfl_sync(0xffffffffu, X.b.x, from), __shfl_sync(0xffffffffu, X.b.y, from));
+    r.c = c2(__shfl_sync(0xffffffffu, X.c.x, from), __shfl_sync(0xffffffffu, X.c.y, from));
+    r.d = c2(__shfl_sync(0xffffffffu, X.d.x, from), __shfl_sync(0xffffffffu, X.d.y, from));
+    return r;
+}
+
+// The Galerkin row m of the term (r1, r2, r3 of M + p D) from the f-window.
+struct Rrow {
+    double2 r1, r2, r3;
+};
+
+// Thomas factorisation of every active term's (M + p D), top-down, all rows
+// of the slice in parallel.  w_m = r3_m / (r2_m - r1_m w_{m-1}) (w_0 = 0) is
+// linear in homogeneous coordinates: (N, D)_m = T_m (N, D)_{m-1} with
+// T_m = [[0, r3], [-r1, r2]] and w = N / D.  So, as for the solves: each
+// segment multiplies its rows' T (sweep A), the warp scans the segments'
+// products, the cluster folds in the slices above, and each segment runs the
+// recurrence from its true entry w (sweep B), storing 1/den, al = -r1/den and
+// w.  All arithmetic is FP64; the factors are stored in the sweep precision.
+// Called by every thread of every CTA (one cluster barrier).
 template <typename R>
-__device__ void col_factor(ColCtx<R>& x, double2 p, int lo) {
-    const int nz = x.nz, R0 = x.sl.R0, R1 = x.sl.R1, k = x.term, P = 32 * x.sl.L;
-    if (x.lane != 0) return;
+__device__ void col_factor(ColCtx<R>& x, const ColSet& cs) {
     const ColArgs& a = *x.a;
+    const int nz = x.nz, k = x.term, l = x.lane, L = x.sl.L, n = x.sl.n, P = 32 * L;
+    const bool active = k < cs.n_active;
+    const double2 p = active ? a.pd2[((long long)x.rid * kSets + cs.set) * CR_MAX_NP + k] : c2(0.0, 0.0);
+    const int p0 = min(n, l * L), p1 = min(n, p0 + L);
     auto ld = [&](int i) {
         EnvRow r;
         if (i < 0 || i > nz + 1) {
@@ -288,37 +339,87 @@ __device__ void col_factor(ColCtx<R>& x, double2 p, int lo) {
         r.k = a.ksq[o];
         return r;
     };
-    double2 wp = c2(0.0, 0.0);
-    int m0 = 1;
-    if (lo > 1 && lo - 1 >= R0 - 1) {
-        m0 = lo;
-        wp = CV<R>::up(lo - 1 == R0 - 1 ? x.sm.wghost[k] : x.sm.W[k * P + x.sl.idx(lo - 1)]);
-    }
-    EnvRow em = ld(m0 - 1), ec = ld(m0), ep;
-    for (int m = m0; m <= R1; ++m) {
-        ep = ld(m + 1);
+    auto row = [&](const EnvRow& em, const EnvRow& ec, const EnvRow& ep) {
         const Drow d = galerkin3(em, ec, ep, x.cfact);
-        const double2 r1 = caxpd(x.a1, p, d.d1), r2 = caxpd(x.a2, p, d.d2), r3 = caxpd(x.a1, p, d.d3);
-        const double2 q = crcp(cfms(r2, r1, wp));
-        wp = cmul(r3, q);
-        if (m >= R0) {
-            const double2 ci = cmul(r1, q);
-            const int o = k * P + x.sl.idx(m);
-            x.sm.Q[o] = CV<R>::mk(q);
-            x.sm.AL[o] = CV<R>::mk(c2(-ci.x, -ci.y));
-            x.sm.W[o] = CV<R>::mk(wp);
-        } else if (m == R0 - 1) {
-            x.sm.wghost[k] = CV<R>::mk(wp);
+        return Rrow{caxpd(x.a1, p, d.d1), caxpd(x.a2, p, d.d2), caxpd(x.a1, p, d.d3)};
+    };
+    M2 Mseg = m2_eye(), ex = m2_eye();
+    if (active) {
+        // sweep A: T of the segment's rows, last row leftmost
+        EnvRow em = ld(x.sl.R0 + p0 - 1), ec = ld(x.sl.R0 + p0), ep;
+        int cnt = 0;
+        for (int q = p0; q < p1; ++q) {
+            const int m = x.sl.R0 + q;
+            ep = ld(m + 1);
+            const Rrow rr = row(em, ec, ep);
+            const M2 T{c2(0.0, 0.0), rr.r3, c2(-rr.r1.x, -rr.r1.y), rr.r2};
+            Mseg = m2_mul(T, Mseg);
+            if (++cnt == 8) {
+                Mseg = m2_norm(Mseg);
+                cnt = 0;
+            }
+            em = ec;
+            ec = ep;
         }
-        em = ec;
-        ec = ep;
+        Mseg = m2_norm(Mseg);
+        // warp scan in lane order: the product of the earlier lanes' maps
+#pragma unroll
+        for (int dd = 1; dd < 32; dd <<= 1) {
+            const M2 prev = m2_shfl(Mseg, max(l - dd, 0));
+            if (l >= dd) Mseg = m2_norm(m2_mul(Mseg, prev));
+        }
+        ex = m2_shfl(Mseg, max(l - 1, 0));
+        if (l == 0) ex = m2_eye();
+        if (l == 31) {
+            x.sm.fmat[4 * k + 0] = Mseg.a;
+            x.sm.fmat[4 * k + 1] = Mseg.b;
+            x.sm.fmat[4 * k + 2] = Mseg.c;
+            x.sm.fmat[4 * k + 3] = Mseg.d;
+        }
     }
+    x.cl->sync();
+    if (active) {
+        // the slices above, in order (lane j holds CTA j's map)
+        M2 C = m2_eye();
+        if (l < x.c) {
+            const double2* f = x.cl->map_shared_rank(x.sm.fmat, l);
+            C = {f[4 * k + 0], f[4 * k + 1], f[4 * k + 2], f[4 * k + 3]};
+        }
+#pragma unroll
+        for (int dd = 1; dd < 16; dd <<= 1) {
+            const M2 prev = m2_shfl(C, max(l - dd, 0));
+            if (l >= dd) C = m2_norm(m2_mul(C, prev));
+        }
+        C = m2_shfl(C, max(x.c - 1, 0));
+        if (x.c == 0) C = m2_eye();
+        // entry (N, D) of this lane's segment: ex C (0, 1)
+        const M2 E = m2_mul(ex, C);
+        const double2 N = E.b, D = E.d;
+        double2 wp = (N.x == 0.0 && N.y == 0.0) ? c2(0.0, 0.0) : cmul(N, crcp(D));
+        if (l == 0) x.sm.wghost[k] = CV<R>::mk(wp);  // w of row R0 - 1
+        // sweep B: the recurrence from the true entry
+        EnvRow em = ld(x.sl.R0 + p0 - 1), ec = ld(x.sl.R0 + p0), ep;
+        int o = l;
+        for (int q = p0; q < p1; ++q, o += 32) {
+            const int m = x.sl.R0 + q;
+            ep = ld(m + 1);
+            const Rrow rr = row(em, ec, ep);
+            const double2 qq = crcp(cfms(rr.r2, rr.r1, wp));
+            wp = cmul(rr.r3, qq);
+            const double2 ci = cmul(rr.r1, qq);
+            x.sm.Q[k * P + o] = CV<R>::mk(qq);
+            x.sm.AL[k * P + o] = CV<R>::mk(c2(-ci.x, -ci.y));
+            x.sm.W[k * P + o] = CV<R>::mk(wp);
+            em = ec;
+            ec = ep;
+        }
+    }
+    __syncthreads();
 }
 
-// Switch to Pade set `ns` (when it changes) and refactor rows lo.. of every
-// active term (all rows on a set change).
+// Switch to Pade set `ns` (when it changes) and refactor every active term.
 template <typename R>
-__device__ __forceinline__ void col_use_set(ColCtx<R>& x, ColSet& cs, int ns, int lo) {
+__device__ __forceinline__ void col_use_set(ColCtx<R>& x, ColSet& cs, int ns) {
     const ColArgs& a = *x.a;
     if (ns != cs.set) {
         cs.set = ns;
@@ -327,13 +428,8 @@ __device__ __forceinline__ void col_use_set(ColCtx<R>& x, ColSet& cs, int ns, in
         if (threadIdx.x < kColMaxTerms)
             x.sm.ck[threadIdx.x] = (int)threadIdx.x < cs.n_active ? a.pfc[base + threadIdx.x] : c2(0.0, 0.0);
         if (threadIdx.x == 0) x.sm.misc[0] = a.pfcinf[(long long)x.rid * kSets + ns];
-        lo = 1;
     }
-    if (x.term < cs.n_active && lo <= x.sl.R1) {
-        const double2 p = a.pd2[((long long)x.rid * kSets + ns) * CR_MAX_NP + x.term];
-        col_factor<R>(x, p, lo);
-    }
-    __syncthreads();
+    col_factor<R>(x, cs);
 }
 
 // One range step of the active set.
@@ -630,10 +726,10 @@ __global__ void __launch_bounds__(32 * kColMaxTerms) march_col_kernel(ColArgs a)
     int mdr = 0, tlc = -1;
 
     // self-starter: two steps of 1/(1-X), one of the ip=2 operator
-    col_use_set(x, cs, 0, 1);
+    col_use_set(x, cs, 0);
     col_step(x, cs);
     col_step(x, cs);
-    col_use_set(x, cs, 1, 1);
+    col_use_set(x, cs, 1);
     col_step(x, cs);
     col_emit(x, mdr, tlc, ir, dir);  // first output at r = dr (cupyram.py:703)
 
@@ -673,9 +769,9 @@ __global__ void __launch_bounds__(32 * kColMaxTerms) march_col_kernel(ColArgs a)
             cl.sync();
             col_load_f3(x, lo, hi);
             iz = iz_new;
-            col_use_set(x, cs, new_set, max(1, lo - 1));
+            col_use_set(x, cs, new_set);
         } else if (new_set != cs.set) {
-            col_use_set(x, cs, new_set, 1);
+            col_use_set(x, cs, new_set);
         }
         col_step(x, cs);
         r = (double)(rn + 2) * ry.dr;

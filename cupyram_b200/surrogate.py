@@ -10,6 +10,13 @@ passes, Adam, all on the GPU.  At inference the members' mean is served
 where they agree; where their spread exceeds 1 dB the request falls back to
 the march.  PyTorch only holds device buffers and streams.
 
+Training fields and fallback fields come from the march's chosen form
+(complex64 sweeps; <= 0.01 dB RMS from complex128 on every measured
+workload, far below the network's own error), whose half-size shared
+footprint lets the column-parallel kernel take the deep, high-frequency
+columns of this distribution.  The judge reruns use the plain complex128
+march.
+
 Coarse field.  Cell (i, j) covers ranges (i, i+1] x 156.25 m and depths
 (j, j+1] x D0 / 64 (D0: water depth at the source).  Its TL is
 -10 log10 of the mean of |p|^2 over a 4 x 4 sub-grid of march outputs in the
@@ -328,7 +335,7 @@ def coarse_tl_host(b, cpg):
     return out
 
 
-def march_tl(q: Requests, chunk=4096, precision="plain"):
+def march_tl(q: Requests, chunk=4096, precision="chosen"):
     """Coarse TL fields of the requests from the march: (tl [n, 64, 128] clipped to [20, 150] dB,
     seconds of march, grid-point updates).  The cells are reduced on the device (Engine.cell_tl)."""
     n = len(q)
@@ -433,11 +440,13 @@ class Served:
     t_net: float            # seconds of network inference (device events)
     t_march: float          # seconds of fallback marches
     march_work: float       # grid-point updates of the fallback marches
+    t_wall: float           # host wall clock of the whole call (features in, fields out)
 
 
 def serve(ens: Ensemble, q: Requests, threshold_db=1.0):
     """Answer requests with the ensemble, falling back to the march where its spread exceeds the threshold."""
     import torch
+    tw = time.perf_counter()
     n = len(q)
     X = to_device_inputs(features(q))
     torch.cuda.synchronize()
@@ -455,7 +464,7 @@ def serve(ens: Ensemble, q: Requests, threshold_db=1.0):
         idx = np.nonzero(fb)[0]
         tl_fb, t_march, work = march_tl(q.take(idx))
         tl[idx] = tl_fb
-    return Served(tl, fb, srms, t_net, t_march, work)
+    return Served(tl, fb, srms, t_net, t_march, work, time.perf_counter() - tw)
 
 
 # ---------------------------------------------------------------------------
@@ -492,7 +501,7 @@ def pipeline(n_train=200_000, n_infer=65_536, judge_frac=0.01, epochs=12, batch=
     t_served = served.t_net + served.t_march
     rng = np.random.Generator(np.random.PCG64(seed + 2))
     idx = np.sort(rng.choice(n_infer, size=max(1, int(round(judge_frac * n_infer))), replace=False))
-    tl_judge, _, _ = march_tl(q.take(idx))
+    tl_judge, _, _ = march_tl(q.take(idx), precision="plain")
     err = served.tl[idx] - tl_judge
     req_rms = np.sqrt(np.mean(err.reshape(len(idx), -1) ** 2, axis=1))
     net_idx = ~served.fallback[idx]
@@ -509,6 +518,8 @@ def pipeline(n_train=200_000, n_infer=65_536, judge_frac=0.01, epochs=12, batch=
         "speedup_vs_march": t_ram_all / t_served,
         "net_only_speedup_vs_march": t_ram_all / max(served.t_net, 1e-12),
         "equivalent_updates_per_s": w_all / t_served,
+        "equivalent_updates_per_s_wall": w_all / served.t_wall,
+        "serve_wall_seconds": served.t_wall,
         "judge_rms_db_mean": float(req_rms.mean()),
         "judge_rms_db_net_served": float(req_rms[net_idx].mean()) if net_idx.any() else None,
         "judge_within_1db": float(np.mean(req_rms <= 1.0)),
