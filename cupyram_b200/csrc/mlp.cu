@@ -14,6 +14,9 @@
 // the tile (M, N of 128, K of 32); the host wrappers check that and the
 // 16-byte alignment of every row.
 //
+// The same contraction also runs on the 5th-generation tensor cores
+// (gemm_tn_umma: tcgen05.mma with the accumulator in tensor memory).
+//
 // Plus the small kernels of a training step: column sums (bias gradients),
 // the masked mean-squared-error gradient, Adam, and BF16 conversion.
 #include <cuda_bf16.h>
@@ -159,6 +162,171 @@ __global__ void __launch_bounds__(kThreads) gemm_tn(const __nv_bfloat16* __restr
         }
 }
 
+// ---------------------------------------------------------------------------
+// The same contraction on the 5th-generation tensor cores (tcgen05).
+//
+// A CTA of 4 warps owns a 128 x 128 block of C; its FP32 accumulator lives in
+// tensor memory (128 lanes x 128 columns).  A and B tiles of 128 rows x 64
+// bf16 (one 128-byte swizzle atom wide) are staged in shared memory by
+// cp.async in the canonical K-major SWIZZLE_128B layout - row r at r x 128
+// bytes, its 16-byte chunk c at chunk c ^ (r mod 8) - over two stages.  One
+// thread issues the four m128 n128 k16 MMAs of a stage and commits them to
+// the stage's mbarrier; the stage is refilled once that barrier flips.  The
+// epilogue reads the accumulator with tcgen05.ld (warp w: lanes 32w..32w+31,
+// i.e. rows 32w..32w+31 of the block) and applies the same epilogues as the
+// mma.sync kernel.  Every wait is bounded: a barrier that does not flip in
+// time sets *err and the kernel finishes without the result.
+// ---------------------------------------------------------------------------
+constexpr int UBM = 128, UBN = 128, UBK = 64;
+constexpr int kUThreads = 128;
+constexpr int kUTile = UBM * UBK * 2;  // bytes of one A (or B) stage tile
+constexpr unsigned kUWaitLimit = 1u << 26;
+
+// Shared-memory matrix descriptor of a K-major SWIZZLE_128B tile (rows of
+// 128 bytes, 8-row atoms 1024 bytes apart): start address and stride byte
+// offset in 16-byte units, descriptor version 1, layout type 2 (128B swizzle).
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)(1) << 16;              // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;      // stride byte offset: next 8-row atom
+    d |= (uint64_t)1 << 46;                // version
+    d |= (uint64_t)2 << 61;                // SWIZZLE_128B
+    return d;
+}
+// Instruction descriptor: D f32, A and B bf16, both K-major, M 128, N 128.
+constexpr uint32_t kUIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(UBN >> 3) << 17) | ((uint32_t)(UBM >> 4) << 24);
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+// true once the barrier's phase with this parity has completed; bounded
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+    for (unsigned it = 0; it < kUWaitLimit; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(kUThreads) gemm_tn_umma(const __nv_bfloat16* __restrict__ A,
+                                                         const __nv_bfloat16* __restrict__ B, int K, int lda, int ldb,
+                                                         EpiArgs e, int* err) {
+    extern __shared__ __align__(1024) unsigned char usmem[];
+    // 1024-byte aligned stage tiles: A0 B0 A1 B1, then barriers and the TMEM address
+    unsigned char* base = (unsigned char*)(((uintptr_t)usmem + 1023) & ~(uintptr_t)1023);
+    auto tA = [&](int st) { return base + st * 2 * kUTile; };
+    auto tB = [&](int st) { return base + kUTile + st * 2 * kUTile; };
+    uint64_t* bar = (uint64_t*)(base + 4 * kUTile);
+    uint32_t* taddr_s = (uint32_t*)(bar + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int bm = blockIdx.y * UBM, bn = blockIdx.x * UBN;
+    const __nv_bfloat16* Ab = A + (size_t)bm * lda;
+    const __nv_bfloat16* Bb = B + (size_t)bn * ldb;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(taddr_s)),
+                     "r"(UBN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *taddr_s;
+
+    auto load = [&](int stage, int k0) {
+        // 128 rows x 8 chunks of 16 bytes per tile, 8 chunks per thread per operand
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int c = tid + i * kUThreads;
+            const int row = c >> 3, ch = c & 7;
+            const int off = row * 128 + ((ch ^ (row & 7)) << 4);
+            cp_async16(tA(stage) + off, Ab + (size_t)row * lda + k0 + ch * 8);
+            cp_async16(tB(stage) + off, Bb + (size_t)row * ldb + k0 + ch * 8);
+        }
+        cp_commit();
+    };
+
+    const int nk = K / UBK;
+    bool ok = true;
+    load(0, 0);
+    for (int kt = 0; kt < nk; ++kt) {
+        const int st = kt & 1;
+        if (kt + 1 < nk) {
+            // stage st^1 was last read by the MMAs of tile kt-1
+            if (kt >= 1) ok &= mbar_wait(&bar[st ^ 1], ((kt - 1) >> 1) & 1);
+            load(st ^ 1, (kt + 1) * UBK);
+            cp_wait<1>();
+        } else {
+            cp_wait<0>();
+        }
+        // make this thread's shared-memory writes visible to the tensor cores
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sa = smem_u32(tA(st)), sb = smem_u32(tB(st));
+#pragma unroll
+            for (int k = 0; k < UBK / 16; ++k) {
+                // k16 slice: 32 bytes further along the swizzled rows
+                const uint64_t da = umma_desc_sw128(sa + k * 32), db = umma_desc_sw128(sb + k * 32);
+                const uint32_t acc = (kt > 0 || k > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                    :
+                    : "r"(tmem), "l"(da), "l"(db), "r"(kUIdesc), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&bar[st]))
+                         : "memory");
+        }
+    }
+    // all MMAs are done once the last commit's barrier flips
+    ok &= mbar_wait(&bar[(nk - 1) & 1], ((nk - 1) >> 1) & 1);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!ok) {
+        if (lane == 0) atomicExch(err, 1);
+    } else {
+        const int row = bm + warp * 32 + lane;
+#pragma unroll 1
+        for (int cc = 0; cc < UBN; cc += 16) {
+            uint32_t v[16];
+            const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cc;
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+                : "r"(ta));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int j = 0; j < 16; j += 2)
+                store2<EPI>(e, row, bn + cc + j, __uint_as_float(v[j]), __uint_as_float(v[j + 1]));
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(UBN));
+}
+
+constexpr size_t kUSmem = 4 * kUTile + 1024 + 64;
+
 // dst[c][r] = src[r][c] for a rows x cols BF16 matrix (32 x 32 tiles).
 __global__ void transpose_bf16(const __nv_bfloat16* __restrict__ src, int lds, __nv_bfloat16* __restrict__ dst,
                                int ldd, int rows, int cols) {
@@ -260,6 +428,37 @@ int cr_mlp_gemm(int epi, const void* A, const void* B, int M, int N, int K, int 
         case CR_MLP_EPI_RELU_MASK_BF16: gemm_tn<CR_MLP_EPI_RELU_MASK_BF16><<<grid, kThreads, 0, st>>>(a, b, K, lda, ldb, e); break;
         default: return CR_MLP_EBADSHAPE;
     }
+    return cudaGetLastError() == cudaSuccess ? 0 : CR_MLP_ECUDA;
+}
+
+int cr_mlp_gemm_tc(int epi, const void* A, const void* B, int M, int N, int K, int lda, int ldb, void* out, int ldo,
+                   const float* bias, const void* mask, int ldm, int* err, void* stream) {
+    if (M <= 0 || N <= 0 || K <= 0 || M % UBM || N % UBN || K % UBK) return CR_MLP_EBADSHAPE;
+    if (lda < K || ldb < K || lda % 8 || ldb % 8 || ldo < N || ldo % 2 || !aligned16(A) || !aligned16(B) || !out ||
+        !err)
+        return CR_MLP_EBADSHAPE;
+    if ((epi == CR_MLP_EPI_BIAS_RELU_BF16 || epi == CR_MLP_EPI_BIAS_F32) && !bias) return CR_MLP_EBADSHAPE;
+    if (epi == CR_MLP_EPI_RELU_MASK_BF16 && (!mask || ldm < N || ldm % 2)) return CR_MLP_EBADSHAPE;
+    EpiArgs e{out, ldo, bias, (const __nv_bfloat16*)mask, ldm};
+    const dim3 grid(N / UBN, M / UBM);
+    cudaStream_t st = (cudaStream_t)stream;
+    auto a = (const __nv_bfloat16*)A;
+    auto b = (const __nv_bfloat16*)B;
+    cudaError_t ce = cudaSuccess;
+    switch (epi) {
+#define CR_UMMA_CASE(E)                                                                                    \
+    case E:                                                                                                \
+        ce = cudaFuncSetAttribute(gemm_tn_umma<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUSmem); \
+        if (ce == cudaSuccess) gemm_tn_umma<E><<<grid, kUThreads, kUSmem, st>>>(a, b, K, lda, ldb, e, err);      \
+        break;
+        CR_UMMA_CASE(CR_MLP_EPI_BIAS_RELU_BF16)
+        CR_UMMA_CASE(CR_MLP_EPI_BIAS_F32)
+        CR_UMMA_CASE(CR_MLP_EPI_F32)
+        CR_UMMA_CASE(CR_MLP_EPI_RELU_MASK_BF16)
+#undef CR_UMMA_CASE
+        default: return CR_MLP_EBADSHAPE;
+    }
+    if (ce != cudaSuccess) return CR_MLP_ECUDA;
     return cudaGetLastError() == cudaSuccess ? 0 : CR_MLP_ECUDA;
 }
 

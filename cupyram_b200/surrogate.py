@@ -75,7 +75,14 @@ _SIGS = {
                     ctypes.c_longlong, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int,
                     ctypes.c_float, ctypes.c_void_p],
     "cr_mlp_to_bf16": [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_longlong, ctypes.c_void_p],
+    "cr_mlp_gemm_tc": [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                       ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                       ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
 }
+# Contractions with K a multiple of 64 run on the tcgen05 tensor cores
+# (cr_mlp_gemm_tc); the others on the mma.sync kernel (cr_mlp_gemm).
+USE_TCGEN05 = False
+_err = None
 EPI_BIAS_RELU_BF16, EPI_BIAS_F32, EPI_F32, EPI_RELU_MASK_BF16 = 0, 1, 2, 3
 _mlp = None
 
@@ -107,14 +114,30 @@ def _p(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None else None
 
 
-def gemm(epi, A, B, out, bias=None, mask=None):
-    """out = epilogue(A B^T); A [M, K], B [N, K] bf16 (K-contiguous rows)."""
+def tc_error_flag():
+    """The device flag the tcgen05 GEMM sets when one of its bounded waits gives up."""
+    global _err
+    if _err is None:
+        import torch
+        _err = torch.zeros(1, dtype=torch.int32, device="cuda")
+    return _err
+
+
+def gemm(epi, A, B, out, bias=None, mask=None, tc=None):
+    """out = epilogue(A B^T); A [M, K], B [N, K] bf16 (K-contiguous rows).  tc: use the tcgen05 kernel
+    (default: USE_TCGEN05 where K is a multiple of 64)."""
     M, K = A.shape
     N = B.shape[0]
     assert B.shape[1] == K
-    _ok(kernels().cr_mlp_gemm(epi, _p(A), _p(B), M, N, K, A.stride(0), B.stride(0), _p(out), out.stride(0),
-                              _p(bias), _p(mask), mask.stride(0) if mask is not None else 0, _stream()),
-        "cr_mlp_gemm")
+    if tc is None:
+        tc = USE_TCGEN05 and K % 64 == 0
+    ldm = mask.stride(0) if mask is not None else 0
+    if tc:
+        _ok(kernels().cr_mlp_gemm_tc(epi, _p(A), _p(B), M, N, K, A.stride(0), B.stride(0), _p(out), out.stride(0),
+                                     _p(bias), _p(mask), ldm, _p(tc_error_flag()), _stream()), "cr_mlp_gemm_tc")
+    else:
+        _ok(kernels().cr_mlp_gemm(epi, _p(A), _p(B), M, N, K, A.stride(0), B.stride(0), _p(out), out.stride(0),
+                                  _p(bias), _p(mask), ldm, _stream()), "cr_mlp_gemm")
 
 
 def transpose(src, dst):
