@@ -67,10 +67,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--form", choices=["plain", "chosen"], default="plain")
-    ap.add_argument("--config", choices=["munk", "pekeris", "wedge", "precision", "surrogate"], default="munk")
+    ap.add_argument("--config", choices=["munk", "pekeris", "wedge", "precision", "surrogate", "gemm"], default="munk")
     ap.add_argument("--train", type=int, default=200_000, help="surrogate: training marches")
     ap.add_argument("--infer", type=int, default=65_536, help="surrogate: served requests")
-    ap.add_argument("--epochs", type=int, default=12, help="surrogate: training epochs per member")
+    ap.add_argument("--epochs", type=int, default=60, help="surrogate: training epochs per member")
     ap.add_argument("--rays", type=int, default=0, help="rays per GPU (0: the configuration's own count)")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -325,10 +325,67 @@ def run_surrogate(a):
     return 0
 
 
+def measured_peak_bf16():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["bf16_tflops"]), "measured"
+        except (KeyError, ValueError):
+            pass
+    return 1590.0, "fallback"
+
+
+def run_gemm(a):
+    """The surrogate's contraction on its inference shape (8192 x 8192 x 512, the last layer of a batch of
+    8192 requests), tcgen05 and mma.sync kernels, TFLOP/s against the measured bf16 peak."""
+    rank, world, local = dist_env()
+    if rank != 0:
+        return 0
+    import torch
+    torch.cuda.set_device(local)
+    from cupyram_b200 import surrogate as S
+    M, N, K = 8192, 8192, 512
+    g = torch.Generator(device="cuda").manual_seed(a.seed)
+    A = torch.randn(M, K, device="cuda", generator=g).to(torch.bfloat16)
+    B = torch.randn(N, K, device="cuda", generator=g).to(torch.bfloat16)
+    bias = torch.zeros(N, device="cuda")
+    out = torch.empty(M, N, device="cuda")
+    flop = 2.0 * M * N * K
+    peak, kind = measured_peak_bf16()
+    res = {}
+    for name, tc in (("tcgen05", True), ("mma.sync", False)):
+        for _ in range(a.warmup):
+            S.gemm(S.EPI_BIAS_F32, A, B, out, bias=bias, tc=tc)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(a.steps):
+            S.gemm(S.EPI_BIAS_F32, A, B, out, bias=bias, tc=tc)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / a.steps
+        res[name] = {"ms": ms, "tflops": flop / ms * 1e-9}
+    assert int(S.tc_error_flag().item()) == 0
+    t = res["tcgen05"]["tflops"]
+    line = {"metric": "surrogate GEMM TFLOP/s (bf16 x bf16 -> f32, 8192 x 8192 x 512)", "value": t,
+            "unit": "TFLOP/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": res["tcgen05"]["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16", "data": "synthetic (random matrices)",
+            "config": {"workload": "surrogate last-layer contraction, batch of 8192 requests", "config": "gemm",
+                       "l2": "operands 16 MB (L2-resident); output 268 MB"},
+            "roofline": {"bound": "tensor", "achieved": t, "peak": peak, "unit": "TFLOP/s", "frac": t / peak,
+                         "peak_source": kind, "traffic": None},
+            "kernels": res}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     a = parse()
     if a.config == "surrogate":
         return run_surrogate(a)
+    if a.config == "gemm":
+        return run_gemm(a)
     if a.impl == "reference":
         return run_reference(a)
     rank, world, local = dist_env()

@@ -81,7 +81,7 @@ _SIGS = {
 }
 # Contractions with K a multiple of 64 run on the tcgen05 tensor cores
 # (cr_mlp_gemm_tc); the others on the mma.sync kernel (cr_mlp_gemm).
-USE_TCGEN05 = False
+USE_TCGEN05 = True
 _err = None
 EPI_BIAS_RELU_BF16, EPI_BIAS_F32, EPI_F32, EPI_RELU_MASK_BF16 = 0, 1, 2, 3
 _mlp = None
@@ -390,7 +390,9 @@ def default_dims(width=512, layers=4):
 
 
 class Ensemble:
-    """Members trained from different initialisations and sample orders."""
+    """Members trained from different initialisations, each on its own
+    bootstrap resample of the training fields (so that their spread reflects
+    the data's uncertainty, not only the initialisation)."""
 
     def __init__(self, n_models=4, dims=None, seed=0):
         self.models = [MLP(dims or default_dims(), seed=seed + 7919 * k) for k in range(n_models)]
@@ -407,9 +409,10 @@ class Ensemble:
         losses = []
         for k, m in enumerate(self.models):
             g = torch.Generator(device=dev).manual_seed(int(seed) * 1000 + k)
+            boot = torch.randint(0, n, (n,), generator=g, device=dev)
             step = 0
             for ep in range(epochs):
-                perm = torch.randperm(n, generator=g, device=dev)
+                perm = boot[torch.randperm(n, generator=g, device=dev)]
                 sse.zero_()
                 for s in range(steps_per_epoch):
                     idx = perm[s * batch:(s + 1) * batch]
@@ -493,7 +496,7 @@ def serve(ens: Ensemble, q: Requests, threshold_db=1.0):
 # ---------------------------------------------------------------------------
 # the whole pipeline (bench.py --config surrogate)
 # ---------------------------------------------------------------------------
-def pipeline(n_train=200_000, n_infer=65_536, judge_frac=0.01, epochs=12, batch=512, lr=1e-3, n_models=4,
+def pipeline(n_train=200_000, n_infer=65_536, judge_frac=0.01, epochs=60, batch=512, lr=1e-3, n_models=4,
              width=512, layers=4, threshold_db=1.0, seed=2024, log=print):
     """Generate the training fields with the march, train the ensemble with the
     tensor-core kernels, serve n_infer seeded requests with fallback, and judge
@@ -546,6 +549,9 @@ def pipeline(n_train=200_000, n_infer=65_536, judge_frac=0.01, epochs=12, batch=
         "judge_rms_db_mean": float(req_rms.mean()),
         "judge_rms_db_net_served": float(req_rms[net_idx].mean()) if net_idx.any() else None,
         "judge_within_1db": float(np.mean(req_rms <= 1.0)),
+        "judge_rms_db_fallback_served": float(req_rms[~net_idx].mean()) if (~net_idx).any() else None,
+        "judge_spread_db_net_served": float(served.spread_db[idx][net_idx].mean()) if net_idx.any() else None,
+        "gemm": "tcgen05" if USE_TCGEN05 else "mma.sync",
         "judge_max_abs_db": float(np.abs(err).max()),
     }
     log(str(res))
