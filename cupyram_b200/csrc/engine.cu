@@ -944,13 +944,17 @@ double operator_changes(const cr_batch* b, const cr_ray& r) {
 // Rays marched by the column-parallel kernel instead of the batched one.
 // A ray's lockstep march in a batched tile takes about (nz + 2)(nr + 4)
 // row steps of one warp in sequence; when that alone exceeds the time the
-// whole batch needs at the batched kernel's throughput, the ray would set
-// the launch's length, and a cluster of SMs marches it instead.  A ray must
+// whole batch needs at the batched kernel's throughput by a margin, the ray
+// would set the launch's length, and a cluster of SMs marches it instead.  A ray must
 // fit the shared memory of a cluster of at most 16 CTAs.  CUPYRAM_B200_COL:
 // 0 never, 1 every ray that fits, unset / other: this rule.
 std::vector<char> pick_column_rays(const cr_batch* b, const std::vector<int>& pd_n, bool chosen) {
     constexpr double kRowStepSeconds = 0.3e-6;    // batched tile, one row of one step
     constexpr double kUpdatesPerSecond = 1.3e10;  // batched kernel, whole GPU
+    // a ray leaves the batched kernel only when it would clearly outlast the
+    // batch: in a homogeneous batch every ray's march is close to the
+    // balanced time, and the batched kernel is the efficient one there
+    constexpr double kMargin = 1.25;
     std::vector<char> col((size_t)b->n_rays, 0);
     const char* env = getenv("CUPYRAM_B200_COL");
     const int mode = (env && env[0] == '0') ? 0 : ((env && env[0] == '1') ? 1 : 2);
@@ -965,7 +969,7 @@ std::vector<char> pick_column_rays(const cr_batch* b, const std::vector<int>& pd
         // batched march about four more passes: back-substitution alone, two
         // factorisation passes, elimination alone
         const double steps = (double)(r.nr + 4) + 4.0 * operator_changes(b, r);
-        if (mode == 2 && (double)(r.nz + 2) * steps * kRowStepSeconds <= tau) continue;
+        if (mode == 2 && (double)(r.nz + 2) * steps * kRowStepSeconds <= kMargin * tau) continue;
         const int terms = col_terms(pd_n, i);
         const int cluster = crk::col_cluster_size(r.nz, terms, chosen);
         if (cluster == 0) continue;

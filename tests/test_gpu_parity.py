@@ -107,6 +107,16 @@ def test_column_march_deep_columns_vs_oracle(cuda_device, monkeypatch, rays):
     assert np.abs(out["tll"][:n] - bat["tll"][:n]).max() < TOL_ORACLE
 
 
+def test_homogeneous_batch_stays_on_the_batched_kernel(cuda_device):
+    """The 4096-ray Munk batch: every ray's lockstep march is close to the
+    batch's balanced time, so the default policy keeps all of them on the
+    batched kernel (engine creation only, no march)."""
+    from cupyram_b200 import workloads
+    b = workloads.build(*workloads.munk_batch(4096, seed=2024), compute_grids=False)
+    with Engine(b) as eng:
+        assert eng.stats()["column_rays"] == 0
+
+
 def test_ram_v15_vs_fortran(cuda_device):
     args, kw, _ = load_case("ram_v15")
     res = CuPyRAM(*args, **kw).run()
