@@ -89,6 +89,20 @@ __device__ __forceinline__ void store2(const EpiArgs& e, int row, int col, float
 }
 
 template <int EPI>
+__device__ __forceinline__ void store1(const EpiArgs& e, int row, int col, float v) {
+    if (EPI == CR_MLP_EPI_BIAS_RELU_BF16) {
+        ((__nv_bfloat16*)e.out)[(size_t)row * e.ldo + col] = __float2bfloat16_rn(fmaxf(v + e.bias[col], 0.f));
+    } else if (EPI == CR_MLP_EPI_BIAS_F32) {
+        ((float*)e.out)[(size_t)row * e.ldo + col] = v + e.bias[col];
+    } else if (EPI == CR_MLP_EPI_F32) {
+        ((float*)e.out)[(size_t)row * e.ldo + col] = v;
+    } else {  // CR_MLP_EPI_RELU_MASK_BF16
+        const float m = __bfloat162float(e.mask[(size_t)row * e.ldm + col]);
+        ((__nv_bfloat16*)e.out)[(size_t)row * e.ldo + col] = __float2bfloat16_rn(m > 0.f ? v : 0.f);
+    }
+}
+
+template <int EPI>
 __global__ void __launch_bounds__(kThreads) gemm_tn(const __nv_bfloat16* __restrict__ A,
                                                      const __nv_bfloat16* __restrict__ B, int K, int lda, int ldb,
                                                      EpiArgs e) {
@@ -165,21 +179,25 @@ __global__ void __launch_bounds__(kThreads) gemm_tn(const __nv_bfloat16* __restr
 // ---------------------------------------------------------------------------
 // The same contraction on the 5th-generation tensor cores (tcgen05).
 //
-// A CTA of 4 warps owns a 128 x 128 block of C; its FP32 accumulator lives in
-// tensor memory (128 lanes x 128 columns).  A and B tiles of 128 rows x 64
-// bf16 (one 128-byte swizzle atom wide) are staged in shared memory by
+// A CTA of 4 warps owns a 128 x 256 block of C; its FP32 accumulator lives in
+// tensor memory (128 lanes x 256 columns, so two CTAs share an SM's 512).  A
+// tiles of 128 rows and B tiles of 256 rows x 64 bf16 (one 128-byte swizzle
+// atom wide) are staged in shared memory by
 // cp.async in the canonical K-major SWIZZLE_128B layout - row r at r x 128
 // bytes, its 16-byte chunk c at chunk c ^ (r mod 8) - over two stages.  One
-// thread issues the four m128 n128 k16 MMAs of a stage and commits them to
+// thread issues the four m128 n256 k16 MMAs of a stage and commits them to
 // the stage's mbarrier; the stage is refilled once that barrier flips.  The
 // epilogue reads the accumulator with tcgen05.ld (warp w: lanes 32w..32w+31,
-// i.e. rows 32w..32w+31 of the block) and applies the same epilogues as the
-// mma.sync kernel.  Every wait is bounded: a barrier that does not flip in
+// i.e. rows 32w..32w+31 of the block), transposes 32 x 32 pieces through
+// shared memory so that each store writes 32 consecutive columns of one row,
+// and applies the same epilogues as the mma.sync kernel.  Every wait is bounded: a barrier that does not flip in
 // time sets *err and the kernel finishes without the result.
 // ---------------------------------------------------------------------------
-constexpr int UBM = 128, UBN = 128, UBK = 64;
+constexpr int UBM = 128, UBN = 256, UBK = 64;
 constexpr int kUThreads = 128;
-constexpr int kUTile = UBM * UBK * 2;  // bytes of one A (or B) stage tile
+constexpr int kUTileA = UBM * UBK * 2;      // bytes of one stage's A tile
+constexpr int kUTileB = UBN * UBK * 2;      // bytes of one stage's B tile
+constexpr int kUStage = kUTileA + kUTileB;  // multiple of 1024
 constexpr unsigned kUWaitLimit = 1u << 26;
 
 // Shared-memory matrix descriptor of a K-major SWIZZLE_128B tile (rows of
@@ -223,9 +241,9 @@ __global__ void __launch_bounds__(kUThreads) gemm_tn_umma(const __nv_bfloat16* _
     extern __shared__ __align__(1024) unsigned char usmem[];
     // 1024-byte aligned stage tiles: A0 B0 A1 B1, then barriers and the TMEM address
     unsigned char* base = (unsigned char*)(((uintptr_t)usmem + 1023) & ~(uintptr_t)1023);
-    auto tA = [&](int st) { return base + st * 2 * kUTile; };
-    auto tB = [&](int st) { return base + kUTile + st * 2 * kUTile; };
-    uint64_t* bar = (uint64_t*)(base + 4 * kUTile);
+    auto tA = [&](int st) { return base + st * kUStage; };
+    auto tB = [&](int st) { return base + st * kUStage + kUTileA; };
+    uint64_t* bar = (uint64_t*)(base + 2 * kUStage);
     uint32_t* taddr_s = (uint32_t*)(bar + 2);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int bm = blockIdx.y * UBM, bn = blockIdx.x * UBN;
@@ -248,14 +266,18 @@ __global__ void __launch_bounds__(kUThreads) gemm_tn_umma(const __nv_bfloat16* _
     const uint32_t tmem = *taddr_s;
 
     auto load = [&](int stage, int k0) {
-        // 128 rows x 8 chunks of 16 bytes per tile, 8 chunks per thread per operand
+        // rows of 8 chunks of 16 bytes: A 128 rows (8 chunks per thread), B 256 rows (16)
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const int c = tid + i * kUThreads;
             const int row = c >> 3, ch = c & 7;
-            const int off = row * 128 + ((ch ^ (row & 7)) << 4);
-            cp_async16(tA(stage) + off, Ab + (size_t)row * lda + k0 + ch * 8);
-            cp_async16(tB(stage) + off, Bb + (size_t)row * ldb + k0 + ch * 8);
+            cp_async16(tA(stage) + row * 128 + ((ch ^ (row & 7)) << 4), Ab + (size_t)row * lda + k0 + ch * 8);
+        }
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const int c = tid + i * kUThreads;
+            const int row = c >> 3, ch = c & 7;
+            cp_async16(tB(stage) + row * 128 + ((ch ^ (row & 7)) << 4), Bb + (size_t)row * ldb + k0 + ch * 8);
         }
         cp_commit();
     };
@@ -303,21 +325,32 @@ __global__ void __launch_bounds__(kUThreads) gemm_tn_umma(const __nv_bfloat16* _
     if (!ok) {
         if (lane == 0) atomicExch(err, 1);
     } else {
-        const int row = bm + warp * 32 + lane;
+        // 32 columns at a time: lane l reads row 32w + l from tensor memory,
+        // the warp transposes the 32 x 32 piece through shared memory (the
+        // stage tiles are idle now) and writes it one row per instruction,
+        // 32 consecutive columns, so that every store fills whole sectors
+        float* stg = reinterpret_cast<float*>(base) + warp * 32 * 33;
 #pragma unroll 1
-        for (int cc = 0; cc < UBN; cc += 16) {
-            uint32_t v[16];
-            const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cc;
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
-                "[%16];"
-                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
-                : "r"(ta));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        for (int cc = 0; cc < UBN; cc += 32) {
 #pragma unroll
-            for (int j = 0; j < 16; j += 2)
-                store2<EPI>(e, row, bn + cc + j, __uint_as_float(v[j]), __uint_as_float(v[j + 1]));
+            for (int h = 0; h < 2; ++h) {
+                uint32_t v[16];
+                const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cc + 16 * h);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                    "[%16];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                      "=r"(v[15])
+                    : "r"(ta));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int j = 0; j < 16; ++j) stg[lane * 33 + 16 * h + j] = __uint_as_float(v[j]);
+            }
+            __syncwarp();
+#pragma unroll 4
+            for (int r = 0; r < 32; ++r) store1<EPI>(e, bm + warp * 32 + r, bn + cc + lane, stg[r * 33 + lane]);
+            __syncwarp();
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -325,7 +358,7 @@ __global__ void __launch_bounds__(kUThreads) gemm_tn_umma(const __nv_bfloat16* _
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(UBN));
 }
 
-constexpr size_t kUSmem = 4 * kUTile + 1024 + 64;
+constexpr size_t kUSmem = 2 * kUStage + 1024 + 64;
 
 // dst[c][r] = src[r][c] for a rows x cols BF16 matrix (32 x 32 tiles).
 __global__ void transpose_bf16(const __nv_bfloat16* __restrict__ src, int lds, __nv_bfloat16* __restrict__ dst,

@@ -79,8 +79,8 @@ _SIGS = {
                        ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
                        ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p],
 }
-# Contractions with K a multiple of 64 run on the tcgen05 tensor cores
-# (cr_mlp_gemm_tc); the others on the mma.sync kernel (cr_mlp_gemm).
+# Contractions with N a multiple of 256 and K of 64 run on the tcgen05 tensor
+# cores (cr_mlp_gemm_tc); the others on the mma.sync kernel (cr_mlp_gemm).
 USE_TCGEN05 = True
 _err = None
 EPI_BIAS_RELU_BF16, EPI_BIAS_F32, EPI_F32, EPI_RELU_MASK_BF16 = 0, 1, 2, 3
@@ -125,12 +125,12 @@ def tc_error_flag():
 
 def gemm(epi, A, B, out, bias=None, mask=None, tc=None):
     """out = epilogue(A B^T); A [M, K], B [N, K] bf16 (K-contiguous rows).  tc: use the tcgen05 kernel
-    (default: USE_TCGEN05 where K is a multiple of 64)."""
+    (default: USE_TCGEN05 where N is a multiple of 256 and K of 64)."""
     M, K = A.shape
     N = B.shape[0]
     assert B.shape[1] == K
     if tc is None:
-        tc = USE_TCGEN05 and K % 64 == 0
+        tc = USE_TCGEN05 and N % 256 == 0 and K % 64 == 0
     ldm = mask.stride(0) if mask is not None else 0
     if tc:
         _ok(kernels().cr_mlp_gemm_tc(epi, _p(A), _p(B), M, N, K, A.stride(0), B.stride(0), _p(out), out.stride(0),

@@ -43,7 +43,7 @@ int cr_mlp_gemm(int epi, const void* A, const void* B, int M, int N, int K, int 
 
 /* cr_mlp_gemm on the 5th-generation tensor cores (tcgen05.mma, FP32
  * accumulator in tensor memory).  Same operands, epilogues and alignment
- * rules; K must be a multiple of 64.  err: a device int that the kernel sets
+ * rules; N must be a multiple of 256 and K of 64.  err: a device int that the kernel sets
  * to 1 if one of its (bounded) waits on the tensor cores gives up, in which
  * case out is incomplete. */
 int cr_mlp_gemm_tc(int epi, const void* A, const void* B, int M, int N, int K, int lda, int ldb, void* out, int ldo,

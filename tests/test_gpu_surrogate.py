@@ -47,7 +47,7 @@ def test_gemm_tcgen05_vs_numpy(cuda_device):
     import torch
     from cupyram_b200 import surrogate as S
     rng = np.random.default_rng(4)
-    M, N, K = 256, 384, 192
+    M, N, K = 256, 512, 192
     A, B = rng.normal(size=(M, K)), rng.normal(size=(N, K))
     bias = rng.normal(size=N)
     mask = rng.normal(size=(M, N))
