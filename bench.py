@@ -83,6 +83,32 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(pg, values, device="cuda"):
+    """Element-wise maximum of per-rank timings over all ranks (the job lasts as long as its slowest rank)."""
+    if pg is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def sum_over_ranks(pg, value, device="cuda"):
+    """Sum of a per-rank quantity over all ranks."""
+    if pg is None:
+        return float(value)
+    import torch
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def whole_job_rate(updates_all_ranks, steps, t_ms):
+    """Grid-point updates per second of the whole job: every rank marches its own seeded batch of the same
+    number of rays (weak scaling), all of them within the slowest rank's time."""
+    return updates_all_ranks * steps / (t_ms * 1e-3)
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -235,11 +261,7 @@ def chosen_form(a, batch, out_plain, torch, world, pg, barrier, peak):
         eng.run(out)
         ms.append(eng.stats()["march_ms"])
     barrier()
-    t = float(np.sum(ms))
-    if pg is not None:
-        tt = torch.tensor([t], dtype=torch.float64, device="cuda")
-        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
-        t = float(tt[0])
+    t = max_over_ranks(pg, [float(np.sum(ms))])[0]
     emax, erms = tl_errors(refs["tll"], out["tll"].numpy())
     errs = {"tl_err_max_db": emax, "tl_err_rms_db": erms, "tl_err_cells": "TL line, cells with TL < 100 dB"}
     if "tlg" in refs:
@@ -248,7 +270,7 @@ def chosen_form(a, batch, out_plain, torch, world, pg, barrier, peak):
                     tl_grid_cells=int(np.sum(np.isfinite(refs["tlg"]) & (refs["tlg"] < 100.0))))
     eng.close()
     pu = batch.point_updates
-    value = pu * world * a.steps / (t * 1e-3)
+    value = whole_job_rate(sum_over_ranks(pg, pu), a.steps, t)
     per_launch_s = float(np.mean(ms)) * 1e-3
     achieved = pu * B_ALG["chosen"] / per_launch_s / 1e9
     tpp = profiled_traffic("chosen") if a.config == "munk" else None
@@ -422,16 +444,11 @@ def main():
             h2d_b, d2h_b = st["h2d_bytes"], st["d2h_bytes"]
             launches += st["kernel_launches"]
     barrier()
-    t_march = float(np.sum(march_ms))
-    t_e2e = float(np.sum(e2e_ms))
-    if pg is not None:
-        t = torch.tensor([t_march, t_e2e], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        t_march, t_e2e = float(t[0]), float(t[1])
+    t_march, t_e2e = max_over_ranks(pg, [float(np.sum(march_ms)), float(np.sum(e2e_ms))])
     pu = batch.point_updates
-    total = pu * world * a.steps
-    value = total / (t_march * 1e-3)
-    e2e = total / (t_e2e * 1e-3)
+    pu_all = sum_over_ranks(pg, pu)
+    value = whole_job_rate(pu_all, a.steps, t_march)
+    e2e = whole_job_rate(pu_all, a.steps, t_e2e)
     # sanity: every ray's line is finite
     tl = out["tll"].numpy()
     if not np.all(np.isfinite(tl)):
