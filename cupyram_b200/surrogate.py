@@ -530,6 +530,10 @@ def pipeline(n_train=200_000, n_infer=65_536, judge_frac=0.01, epochs=60, batch=
     tl_judge, _, _ = march_tl(q.take(idx), precision="plain")
     err = served.tl[idx] - tl_judge
     req_rms = np.sqrt(np.mean(err.reshape(len(idx), -1) ** 2, axis=1))
+    # the same over the cells the march puts below 100 dB (the precision study's mask)
+    lit = (tl_judge < 100.0).reshape(len(idx), -1)
+    e2 = np.where(lit, err.reshape(len(idx), -1) ** 2, 0.0)
+    req_rms_lit = np.sqrt(e2.sum(axis=1) / np.maximum(lit.sum(axis=1), 1))
     net_idx = ~served.fallback[idx]
     res = {
         "n_train": n_train, "n_infer": n_infer, "n_judge": int(len(idx)), "members": n_models,
@@ -549,6 +553,8 @@ def pipeline(n_train=200_000, n_infer=65_536, judge_frac=0.01, epochs=60, batch=
         "judge_rms_db_mean": float(req_rms.mean()),
         "judge_rms_db_net_served": float(req_rms[net_idx].mean()) if net_idx.any() else None,
         "judge_within_1db": float(np.mean(req_rms <= 1.0)),
+        "judge_rms_db_mean_tl_below_100": float(req_rms_lit.mean()),
+        "judge_within_1db_tl_below_100": float(np.mean(req_rms_lit <= 1.0)),
         "judge_rms_db_fallback_served": float(req_rms[~net_idx].mean()) if (~net_idx).any() else None,
         "judge_spread_db_net_served": float(served.spread_db[idx][net_idx].mean()) if net_idx.any() else None,
         "gemm": "tcgen05" if USE_TCGEN05 else "mma.sync",
