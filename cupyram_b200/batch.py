@@ -110,7 +110,55 @@ def check_inputs(n_env, zs, zr, z_ss, rp_ss, cw, z_sb, rp_sb, cb, rhob, attn, rb
     """Validate every environment; returns the list of EnvRecord (cupyram.py:382-434).
 
     zs / zr are arrays of length n_env (the same value repeated in shared mode).
+    A batch of equal-shaped environments without NaN padding is checked with
+    whole-batch array operations; any other batch, and any batch that fails a
+    check, goes through the per-environment loop, which raises the error.
     """
+    envs = check_uniform(n_env, zs, zr, z_ss, rp_ss, cw, z_sb, rp_sb, cb, rhob, attn, rbzb)
+    if envs is not None:
+        return envs
+    return check_each(n_env, zs, zr, z_ss, rp_ss, cw, z_sb, rp_sb, cb, rhob, attn, rbzb)
+
+
+def check_uniform(n_env, zs, zr, z_ss, rp_ss, cw, z_sb, rp_sb, cb, rhob, attn, rbzb):
+    """The checks of check_each over a whole batch at once, or None.
+
+    Applies when the profiles are stacked [n_env, n] arrays and the tables
+    [n_env, n, m] arrays with no NaN anywhere, so that every valid slice is
+    the whole entry.  Returns None when that does not hold or any check
+    fails (the loop then reports the first failing environment).
+    """
+    vecs = [np.asarray(a) for a in (z_ss, rp_ss, z_sb, rp_sb)]
+    tabs = [np.asarray(a) for a in (cw, cb, rhob, attn, rbzb)]
+    if any(a.ndim != 2 or a.shape[0] != n_env for a in vecs) or \
+            any(a.ndim != 3 or a.shape[0] != n_env for a in tabs):
+        return None
+    if any(not (np.issubdtype(a.dtype, np.floating) or np.issubdtype(a.dtype, np.integer)) for a in vecs + tabs):
+        return None
+    zss, rps, zsb, rpb = (a.astype(np.float64, copy=False) for a in vecs)
+    cwb, cbb, rhb, atb, bt = (a.astype(np.float64, copy=False) for a in tabs)
+    if any(not np.all(np.isfinite(a)) for a in (zss, rps, zsb, rpb, cwb, cbb, rhb, atb, bt)):
+        return None
+    if zss.shape[1] == 0 or rps.shape[1] == 0 or zsb.shape[1] == 0 or rpb.shape[1] == 0 or bt.shape[1] == 0:
+        return None
+    if cwb.shape[1:] != (zss.shape[1], rps.shape[1]) or bt.shape[2] != 2:
+        return None
+    if any(p.shape[1:] != (zsb.shape[1], rpb.shape[1]) for p in (cbb, rhb, atb)):
+        return None
+    zs = np.asarray(zs, dtype=np.float64)
+    zr = np.asarray(zr, dtype=np.float64)
+    top, bottom = zss[:, 0], zss[:, -1]
+    ok = (top <= zs) & (zs <= bottom) & (top <= zr) & (zr <= bottom)
+    ok &= bt[:, :, 1].max(axis=1) <= bottom
+    if not np.all(ok):
+        return None
+    if np.any(cwb <= 0) or np.any(cbb <= 0) or np.any(rhb <= 0):
+        return None
+    return [EnvRecord(zss[b], rps[b], cwb[b], zsb[b], rpb[b], cbb[b], rhb[b], atb[b], bt[b]) for b in range(n_env)]
+
+
+def check_each(n_env, zs, zr, z_ss, rp_ss, cw, z_sb, rp_sb, cb, rhob, attn, rbzb):
+    """check_inputs one environment at a time (NaN-padded or ragged batches)."""
     envs = []
     for b in range(n_env):
         zss = valid_slice(z_ss[b])[0].astype(np.float64)
@@ -266,6 +314,82 @@ def derive_params(envs, freqs, per_ray, kwargs, np_default=8, dzf=0.1, ndr_defau
                   zmplt, rmax, ns, rs, lyrw, lam, kwargs.get("id", id_default))
 
 
+def pack_pool(envs, zsb_abs, bt_ext):
+    """cr_env records and the float64 pool; per environment the sections
+    z_ss, rp_ss, cw[n_rss][n_zss], z_sb (absolute), rp_sb, cb, rhob, attn
+    (each [n_rsb][n_zsb]), rb, zb, laid end to end from record.off.
+
+    Equal-shaped environments (the extended bathymetry may still differ by
+    its last point) are packed by one scatter; others one at a time.
+    """
+    n_env = len(envs)
+    env_arr = np.zeros(n_env, dtype=ENV_DTYPE)
+    if n_env == 0:
+        return env_arr, np.zeros(1)
+    shape0 = tuple(getattr(envs[0], f).shape for f in ("z_ss", "rp_ss", "z_sb", "rp_sb", "rbzb"))
+    uniform = all(tuple(getattr(e, f).shape for f in ("z_ss", "rp_ss", "z_sb", "rp_sb", "rbzb")) == shape0
+                  for e in envs)
+    uniform = uniform and all(b.shape[0] - e.rbzb.shape[0] in (0, 1) for e, b in zip(envs, bt_ext))
+    if not uniform:
+        return _pack_each(envs, zsb_abs, bt_ext, env_arr)
+    front = np.concatenate([np.stack([e.z_ss for e in envs]), np.stack([e.rp_ss for e in envs]),
+                            np.stack([e.cw.T.reshape(-1) for e in envs]), np.stack(zsb_abs),
+                            np.stack([e.rp_sb for e in envs]), np.stack([e.cb.T.reshape(-1) for e in envs]),
+                            np.stack([e.rhob.T.reshape(-1) for e in envs]),
+                            np.stack([e.attn.T.reshape(-1) for e in envs])], axis=1).astype(np.float64, copy=False)
+    n_front = front.shape[1]
+    bt = np.stack([e.rbzb for e in envs]).astype(np.float64, copy=False)  # [n_env, n_bt, 2]
+    n_bt = bt.shape[1]
+    ext = np.array([b.shape[0] > n_bt for b in bt_ext])
+    n_bt_k = n_bt + ext.astype(np.int64)
+    size = n_front + 2 * n_bt_k
+    off = np.cumsum(size) - size
+    pool = np.empty(int(size.sum()))
+    pool[off[:, None] + np.arange(n_front)] = front
+    rb0 = off + n_front
+    zb0 = rb0 + n_bt_k
+    pool[rb0[:, None] + np.arange(n_bt)] = bt[:, :, 0]
+    pool[zb0[:, None] + np.arange(n_bt)] = bt[:, :, 1]
+    if ext.any():
+        last = np.array([b[-1] for b, x in zip(bt_ext, ext) if x])
+        pool[rb0[ext] + n_bt] = last[:, 0]
+        pool[zb0[ext] + n_bt] = last[:, 1]
+    env_arr["n_zss"], env_arr["n_rss"] = shape0[0][0], shape0[1][0]
+    env_arr["n_zsb"], env_arr["n_rsb"] = shape0[2][0], shape0[3][0]
+    env_arr["n_bt"] = n_bt_k
+    env_arr["off"] = off
+    return env_arr, pool
+
+
+def _pack_each(envs, zsb_abs, bt_ext, env_arr):
+    chunks = []
+    off = 0
+    for k, e in enumerate(envs):
+        parts = [e.z_ss, e.rp_ss, e.cw.T.reshape(-1), zsb_abs[k], e.rp_sb, e.cb.T.reshape(-1),
+                 e.rhob.T.reshape(-1), e.attn.T.reshape(-1), bt_ext[k][:, 0], bt_ext[k][:, 1]]
+        env_arr[k] = (e.z_ss.size, e.rp_ss.size, zsb_abs[k].size, e.rp_sb.size, bt_ext[k].shape[0], 0, off)
+        for q in parts:
+            chunks.append(np.ascontiguousarray(q, dtype=np.float64))
+            off += q.size
+    return env_arr, np.concatenate(chunks)
+
+
+def output_axis(n, d, nd):
+    """Output ranges (or depths) (1..n_b) * d_b * nd_b of every calculation b, one array each."""
+    n = np.asarray(n, dtype=np.int64)
+    d = np.asarray(d, dtype=np.float64)
+    nd = np.asarray(nd)
+    out = [None] * n.size
+    order = np.argsort(n, kind="stable")
+    for idx in np.split(order, np.flatnonzero(np.diff(n[order])) + 1):
+        if idx.size == 0:
+            continue
+        rows = np.arange(1, n[idx[0]] + 1)[None, :] * d[idx, None] * nd[idx, None]
+        for j, b in enumerate(idx):
+            out[b] = rows[j]
+    return out
+
+
 def build_batch(envs, p: Params, zs, zr, per_ray, compute_grids):
     """Grid sizes, output sizes and the packed C-ABI arrays (cupyram.py:528-726).
 
@@ -299,59 +423,49 @@ def build_batch(envs, p: Params, zs, zr, per_ray, compute_grids):
     if np.any(nvr < 1) or np.any(nr < 0):
         raise ValueError("rmax must cover at least one output range step")
 
-    # pool: per env  z_ss, rp_ss, cw[n_rss][n_zss], z_sb, rp_sb, cb, rhob, attn, rb, zb
-    env_arr = np.zeros(n_env, dtype=ENV_DTYPE)
-    chunks = []
-    off = 0
-    for k, e in enumerate(envs):
-        parts = [e.z_ss, e.rp_ss, e.cw.T.reshape(-1), zsb_abs[k], e.rp_sb, e.cb.T.reshape(-1),
-                 e.rhob.T.reshape(-1), e.attn.T.reshape(-1), bt_ext[k][:, 0], bt_ext[k][:, 1]]
-        env_arr[k] = (e.z_ss.size, e.rp_ss.size, zsb_abs[k].size, e.rp_sb.size, bt_ext[k].shape[0], 0, off)
-        for q in parts:
-            chunks.append(np.ascontiguousarray(q, dtype=np.float64))
-            off += q.size
-    pool = np.concatenate(chunks) if chunks else np.zeros(1)
+    env_arr, pool = pack_pool(envs, zsb_abs, bt_ext)
 
+    e_of = np.arange(n_calc) // n_freq
+    zs = np.asarray(zs, dtype=np.float64)
+    zr = np.asarray(zr, dtype=np.float64)
     rays = np.zeros(n_calc, dtype=RAY_DTYPE)
-    line_off = 0
-    grid_off = 0
-    for b in range(n_calc):
-        e = b // n_freq
-        f = p.freqs[b] if per_ray else p.freqs[b % n_freq]
-        r = rays[b]
-        r["freq"] = f
-        r["c0"] = p.c0_env[e]
-        r["zs"] = zs[e]
-        r["zr"] = zr[e]
-        r["dz"] = p.dz[b]
-        r["dr"] = p.dr[b]
-        r["zmax"] = zmax[b]
-        r["lyrw_lambda"] = p.lyrw * p.lam[b]
-        r["attnf"] = ATTNF
-        r["rs"] = p.rs[b]
-        r["nz"] = nz[b]
-        r["nr"] = nr[b]
-        r["np"] = p.np_pade[b]
-        r["ns"] = p.ns
-        r["ndr"] = p.ndr[b] if np.ndim(p.ndr) else p.ndr
-        r["ndz"] = p.ndz[b] if np.ndim(p.ndz) else p.ndz
-        r["nvr"] = nvr[b]
-        r["nvz"] = nvz[b]
-        r["env"] = e
-        r["line_off"] = line_off
-        line_off += int(nvr[b])
-        if compute_grids:
-            r["grid_off"] = grid_off
-            grid_off += int(nvz[b] * nvr[b])
-        else:
-            r["grid_off"] = -1
-    for b in range(n_calc):
-        if int(np.floor(zs[b // n_freq] / p.dz[b])) + 1 > nz[b]:
-            raise ValueError(f"Ray {b}: source depth below the computational grid")
+    rays["freq"] = p.freqs if per_ray else np.tile(p.freqs, n_env)
+    rays["c0"] = p.c0_env[e_of]
+    rays["zs"] = zs[e_of]
+    rays["zr"] = zr[e_of]
+    rays["dz"] = p.dz
+    rays["dr"] = p.dr
+    rays["zmax"] = zmax
+    rays["lyrw_lambda"] = p.lyrw * p.lam
+    rays["attnf"] = ATTNF
+    rays["rs"] = p.rs
+    rays["nz"] = nz
+    rays["nr"] = nr
+    rays["np"] = p.np_pade
+    rays["ns"] = p.ns
     ndr_b = np.broadcast_to(p.ndr, (n_calc,))
     ndz_b = np.broadcast_to(p.ndz, (n_calc,))
-    vr = [np.arange(1, nvr[b] + 1) * p.dr[b] * ndr_b[b] for b in range(n_calc)]
-    vz = [np.arange(1, nvz[b] + 1) * p.dz[b] * ndz_b[b] for b in range(n_calc)]
+    rays["ndr"] = ndr_b
+    rays["ndz"] = ndz_b
+    rays["nvr"] = nvr
+    rays["nvz"] = nvz
+    rays["env"] = e_of
+    ends = np.cumsum(nvr)
+    rays["line_off"] = ends - nvr
+    line_off = int(ends[-1]) if n_calc else 0
+    if compute_grids:
+        cells = nvz * nvr
+        ends = np.cumsum(cells)
+        rays["grid_off"] = ends - cells
+        grid_off = int(ends[-1]) if n_calc else 0
+    else:
+        rays["grid_off"] = -1
+        grid_off = 0
+    below = np.floor(zs[e_of] / p.dz) + 1 > nz
+    if below.any():
+        raise ValueError(f"Ray {int(np.argmax(below))}: source depth below the computational grid")
+    vr = output_axis(nvr, p.dr, ndr_b)
+    vz = output_axis(nvz, p.dz, ndz_b)
     return Batch(rays, env_arr, pool, line_off, grid_off, bool(compute_grids), n_env, n_freq,
                  per_ray, nz, nvr, nvz, zmax, vr, vz)
 

@@ -87,3 +87,76 @@ def test_per_ray_grids():
     assert b.rays["nz"][1] > b.rays["nz"][0]          # finer dz at higher frequency
     assert b.rays["lyrw_lambda"][0] == pytest.approx(20 * 1500.0 / 50.0)
     assert b.rays["lyrw_lambda"][1] == pytest.approx(20 * 1500.0 / 100.0)
+
+
+def _uniform_batch(n, seed, bad=None):
+    """n equal-shaped per-ray environments; about half of the bathymetry lines end
+    short of rmax (so build_batch extends them) and the rest reach beyond it."""
+    rng = np.random.default_rng(seed)
+    depth = rng.uniform(150.0, 400.0, n)
+    z_ss = np.linspace(0.0, 1.0, 6)[None, :] * (depth + 50.0)[:, None]
+    cw = 1500.0 + rng.uniform(-5.0, 5.0, (n, 6, 2))
+    r_end = np.where(rng.random(n) < 0.5, 3000.0, 5000.0)
+    rbzb = np.zeros((n, 3, 2))
+    rbzb[:, 1, 0], rbzb[:, 2, 0] = 1000.0, r_end
+    rbzb[:, :, 1] = depth[:, None] * np.array([1.0, 0.9, 0.8])[None, :]
+    zs = rng.uniform(10.0, 100.0, n)
+    if bad is not None:
+        zs[bad] = z_ss[bad, -1] + 1.0
+    args = [rng.uniform(40.0, 80.0, n), zs, zs * 0.5, list(z_ss), [np.array([0.0, 2000.0])] * n, list(cw),
+            [np.array([0.0, 100.0])] * n, [np.array([0.0])] * n,
+            [np.array([[1700.0], [1800.0]])] * n, [np.array([[1.5], [1.6]])] * n, [np.array([[0.5], [0.5]])] * n,
+            list(rbzb)]
+    return args, dict(batch_size=n, per_ray=True, rmax=4000.0)
+
+
+def test_whole_batch_checks_match_per_environment_loop():
+    args, kw = _uniform_batch(40, 5)
+    norm = [B.normalize_to_batch(x, 40, "x") for x in args[3:]]
+    zs, zr = np.asarray(args[1]), np.asarray(args[2])
+    fast = B.check_uniform(40, zs, zr, *norm)
+    slow = B.check_each(40, zs, zr, *norm)
+    assert fast is not None and len(fast) == len(slow)
+    for a, b in zip(fast, slow):
+        for f in a.__dataclass_fields__:
+            x, y = getattr(a, f), getattr(b, f)
+            assert x.shape == y.shape and np.array_equal(x, y), f
+
+
+def test_whole_batch_pool_matches_per_environment_packing():
+    args, kw = _uniform_batch(40, 6)
+    envs, p, zs, zr, pr = B.prepare(*args, dict(kw))
+    b = B.build_batch(envs, p, zs, zr, pr, True)
+    assert 0 < int(np.sum(b.envs["n_bt"] == 4)) < 40  # both extended and unextended lines
+    zsb_abs = [e.z_sb + e.z_ss[-1] for e in envs]
+    bt_ext = [np.vstack([e.rbzb, [4000.0, e.rbzb[-1, 1]]]) if e.rbzb[-1, 0] < 4000.0 else e.rbzb for e in envs]
+    env_ref, pool_ref = B._pack_each(envs, zsb_abs, bt_ext, np.zeros(len(envs), dtype=b.envs.dtype))
+    assert b.envs.tobytes() == env_ref.tobytes()
+    assert b.pool.tobytes() == pool_ref.tobytes()
+
+
+def test_ray_table_matches_per_ray_restatement():
+    args, kw = _uniform_batch(24, 7)
+    envs, p, zs, zr, pr = B.prepare(*args, dict(kw))
+    b = B.build_batch(envs, p, zs, zr, pr, True)
+    line = grid = 0
+    for k, r in enumerate(b.rays):
+        assert (r["freq"], r["c0"], r["zs"], r["zr"]) == (p.freqs[k], p.c0_env[k], zs[k], zr[k])
+        assert (r["dz"], r["dr"], r["rs"], r["env"]) == (p.dz[k], p.dr[k], p.rs[k], k)
+        assert (r["line_off"], r["grid_off"]) == (line, grid)
+        line += int(r["nvr"])
+        grid += int(r["nvr"]) * int(r["nvz"])
+        assert np.array_equal(b.vr[k], np.arange(1, r["nvr"] + 1) * p.dr[k] * r["ndr"])
+        assert np.array_equal(b.vz[k], np.arange(1, r["nvz"] + 1) * p.dz[k] * r["ndz"])
+    assert (b.line_len, b.grid_len) == (line, grid)
+
+
+def test_whole_batch_errors_name_the_first_bad_ray():
+    args, kw = _uniform_batch(30, 8, bad=17)
+    with pytest.raises(ValueError, match="Ray 17: Source depth"):
+        B.prepare(*args, dict(kw))
+    args, kw = _uniform_batch(30, 8)
+    args[5][4] = args[5][4].copy()
+    args[5][4][2, 1] = -1.0
+    with pytest.raises(ValueError, match="Ray 4: sound speeds"):
+        B.prepare(*args, dict(kw))
