@@ -110,51 +110,86 @@ def check_inputs(n_env, zs, zr, z_ss, rp_ss, cw, z_sb, rp_sb, cb, rhob, attn, rb
     """Validate every environment; returns the list of EnvRecord (cupyram.py:382-434).
 
     zs / zr are arrays of length n_env (the same value repeated in shared mode).
-    A batch of equal-shaped environments without NaN padding is checked with
-    whole-batch array operations; any other batch, and any batch that fails a
-    check, goes through the per-environment loop, which raises the error.
+    A batch of stacked (possibly NaN-padded) arrays is checked with whole-batch
+    array operations; any other batch, and any batch that fails a check, goes
+    through the per-environment loop, which raises the error.
     """
-    envs = check_uniform(n_env, zs, zr, z_ss, rp_ss, cw, z_sb, rp_sb, cb, rhob, attn, rbzb)
+    envs = check_batch(n_env, zs, zr, z_ss, rp_ss, cw, z_sb, rp_sb, cb, rhob, attn, rbzb)
     if envs is not None:
         return envs
     return check_each(n_env, zs, zr, z_ss, rp_ss, cw, z_sb, rp_sb, cb, rhob, attn, rbzb)
 
 
-def check_uniform(n_env, zs, zr, z_ss, rp_ss, cw, z_sb, rp_sb, cb, rhob, attn, rbzb):
+def _lead_len(a):
+    """valid_slice's length for every row of a [B, n] array: up to the first NaN
+    (the whole row when the first entry is NaN, which then fails the checks)."""
+    nan = np.isnan(a)
+    k = np.argmax(nan, axis=1)
+    return np.where(nan.any(axis=1) & (k > 0), k, a.shape[1])
+
+
+def _table_dims(a):
+    """valid_slice's rows and columns for every [n, m] entry of a [B, n, m] array:
+    the counts of rows and of columns that are not entirely NaN."""
+    nan = np.isnan(a)
+    return (~nan.all(axis=2)).sum(axis=1), (~nan.all(axis=1)).sum(axis=1)
+
+
+def check_batch(n_env, zs, zr, z_ss, rp_ss, cw, z_sb, rp_sb, cb, rhob, attn, rbzb):
     """The checks of check_each over a whole batch at once, or None.
 
-    Applies when the profiles are stacked [n_env, n] arrays and the tables
-    [n_env, n, m] arrays with no NaN anywhere, so that every valid slice is
-    the whole entry.  Returns None when that does not hold or any check
-    fails (the loop then reports the first failing environment).
+    Applies when the profiles are [n_env, n] arrays and the tables
+    [n_env, n, m] arrays (as normalize_to_batch stacks or NaN-pads them).
+    Every environment's valid part is found as valid_slice finds it; the
+    records are views of those parts.  Returns None when the layout does
+    not apply or any check fails (the loop then reports the first failing
+    environment).
     """
     vecs = [np.asarray(a) for a in (z_ss, rp_ss, z_sb, rp_sb)]
     tabs = [np.asarray(a) for a in (cw, cb, rhob, attn, rbzb)]
-    if any(a.ndim != 2 or a.shape[0] != n_env for a in vecs) or \
-            any(a.ndim != 3 or a.shape[0] != n_env for a in tabs):
+    if any(a.ndim != 2 or a.shape[0] != n_env or a.shape[1] == 0 for a in vecs) or \
+            any(a.ndim != 3 or a.shape[0] != n_env or 0 in a.shape[1:] for a in tabs):
         return None
     if any(not (np.issubdtype(a.dtype, np.floating) or np.issubdtype(a.dtype, np.integer)) for a in vecs + tabs):
         return None
     zss, rps, zsb, rpb = (a.astype(np.float64, copy=False) for a in vecs)
     cwb, cbb, rhb, atb, bt = (a.astype(np.float64, copy=False) for a in tabs)
-    if any(not np.all(np.isfinite(a)) for a in (zss, rps, zsb, rpb, cwb, cbb, rhb, atb, bt)):
+    n_zss, n_rss, n_zsb, n_rsb = (_lead_len(a) for a in (zss, rps, zsb, rpb))
+    (cw_r, cw_c), (cb_r, cb_c), (rh_r, rh_c), (at_r, at_c), (bt_r, bt_c) = (
+        _table_dims(a) for a in (cwb, cbb, rhb, atb, bt))
+    if not (np.array_equal(cw_r, n_zss) and np.array_equal(cw_c, n_rss)):
         return None
-    if zss.shape[1] == 0 or rps.shape[1] == 0 or zsb.shape[1] == 0 or rpb.shape[1] == 0 or bt.shape[1] == 0:
+    for r, c in ((cb_r, cb_c), (rh_r, rh_c), (at_r, at_c)):
+        if not (np.array_equal(r, n_zsb) and np.array_equal(c, n_rsb)):
+            return None
+    if np.any(bt_c != 2) or np.any(bt_r < 1):
         return None
-    if cwb.shape[1:] != (zss.shape[1], rps.shape[1]) or bt.shape[2] != 2:
-        return None
-    if any(p.shape[1:] != (zsb.shape[1], rpb.shape[1]) for p in (cbb, rhb, atb)):
-        return None
+
+    def vmask(a, n):
+        return np.arange(a.shape[1])[None, :] < n[:, None]
+
+    def tmask(a, r, c):
+        return (np.arange(a.shape[1])[None, :, None] < r[:, None, None]) & \
+               (np.arange(a.shape[2])[None, None, :] < c[:, None, None])
+
+    masks = [vmask(zss, n_zss), vmask(rps, n_rss), vmask(zsb, n_zsb), vmask(rpb, n_rsb),
+             tmask(cwb, cw_r, cw_c), tmask(cbb, cb_r, cb_c), tmask(rhb, rh_r, rh_c), tmask(atb, at_r, at_c),
+             tmask(bt, bt_r, bt_c)]
+    for a, m in zip((zss, rps, zsb, rpb, cwb, cbb, rhb, atb, bt), masks):
+        if not np.all(np.isfinite(a) | ~m):
+            return None
     zs = np.asarray(zs, dtype=np.float64)
     zr = np.asarray(zr, dtype=np.float64)
-    top, bottom = zss[:, 0], zss[:, -1]
+    top, bottom = zss[:, 0], zss[np.arange(n_env), n_zss - 1]
     ok = (top <= zs) & (zs <= bottom) & (top <= zr) & (zr <= bottom)
-    ok &= bt[:, :, 1].max(axis=1) <= bottom
+    ok &= np.where(masks[8][:, :, 1], bt[:, :, 1], -np.inf).max(axis=1) <= bottom
     if not np.all(ok):
         return None
-    if np.any(cwb <= 0) or np.any(cbb <= 0) or np.any(rhb <= 0):
+    if np.any((cwb <= 0) & masks[4]) or np.any((cbb <= 0) & masks[5]) or np.any((rhb <= 0) & masks[6]):
         return None
-    return [EnvRecord(zss[b], rps[b], cwb[b], zsb[b], rpb[b], cbb[b], rhb[b], atb[b], bt[b]) for b in range(n_env)]
+    return [EnvRecord(zss[b, :n_zss[b]], rps[b, :n_rss[b]], cwb[b, :cw_r[b], :cw_c[b]], zsb[b, :n_zsb[b]],
+                      rpb[b, :n_rsb[b]], cbb[b, :cb_r[b], :cb_c[b]], rhb[b, :rh_r[b], :rh_c[b]],
+                      atb[b, :at_r[b], :at_c[b]], bt[b, :bt_r[b], :bt_c[b]]) for b in range(n_env)]
 
 
 def check_each(n_env, zs, zr, z_ss, rp_ss, cw, z_sb, rp_sb, cb, rhob, attn, rbzb):

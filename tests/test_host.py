@@ -114,7 +114,7 @@ def test_whole_batch_checks_match_per_environment_loop():
     args, kw = _uniform_batch(40, 5)
     norm = [B.normalize_to_batch(x, 40, "x") for x in args[3:]]
     zs, zr = np.asarray(args[1]), np.asarray(args[2])
-    fast = B.check_uniform(40, zs, zr, *norm)
+    fast = B.check_batch(40, zs, zr, *norm)
     slow = B.check_each(40, zs, zr, *norm)
     assert fast is not None and len(fast) == len(slow)
     for a, b in zip(fast, slow):
@@ -159,4 +159,55 @@ def test_whole_batch_errors_name_the_first_bad_ray():
     args[5][4] = args[5][4].copy()
     args[5][4][2, 1] = -1.0
     with pytest.raises(ValueError, match="Ray 4: sound speeds"):
+        B.prepare(*args, dict(kw))
+
+
+def _ragged_batch(n, seed):
+    """n per-ray environments whose profiles, tables and bathymetry lines all differ in length."""
+    rng = np.random.default_rng(seed)
+    nzs, nrs, nzb, nrb, nbt = (rng.integers(lo, hi, n) for lo, hi in ((3, 9), (1, 4), (1, 4), (1, 3), (1, 5)))
+    depth = rng.uniform(150.0, 400.0, n)
+    bt = []
+    for i in range(n):
+        r = np.sort(rng.uniform(0.0, 6000.0, nbt[i]))
+        r[0] = 0.0
+        bt.append(np.stack([r, depth[i] * rng.uniform(0.7, 1.0, nbt[i])], axis=1))
+    zs = rng.uniform(10.0, 100.0, n)
+    args = [rng.uniform(40.0, 80.0, n), zs, zs * 0.5,
+            [np.linspace(0.0, depth[i] + 50.0, nzs[i]) for i in range(n)],
+            [np.linspace(0.0, 3000.0, nrs[i]) for i in range(n)],
+            [1500.0 + rng.uniform(-5.0, 5.0, (nzs[i], nrs[i])) for i in range(n)],
+            [np.linspace(0.0, 100.0, nzb[i]) for i in range(n)],
+            [np.linspace(0.0, 2000.0, nrb[i]) for i in range(n)],
+            [rng.uniform(1600.0, 1800.0, (nzb[i], nrb[i])) for i in range(n)],
+            [rng.uniform(1.3, 2.0, (nzb[i], nrb[i])) for i in range(n)],
+            [rng.uniform(0.1, 1.0, (nzb[i], nrb[i])) for i in range(n)], bt]
+    return args, dict(batch_size=n, per_ray=True, rmax=4000.0)
+
+
+def test_padded_batch_checks_match_per_environment_loop():
+    args, kw = _ragged_batch(60, 9)
+    norm = [B.normalize_to_batch(x, 60, "x") for x in args[3:]]
+    assert all(np.isnan(a).any() for a in norm)  # every input is NaN-padded
+    zs, zr = np.asarray(args[1]), np.asarray(args[2])
+    fast = B.check_batch(60, zs, zr, *norm)
+    slow = B.check_each(60, zs, zr, *norm)
+    assert fast is not None
+    for a, b in zip(fast, slow):
+        for f in a.__dataclass_fields__:
+            x, y = getattr(a, f), getattr(b, f)
+            assert x.shape == y.shape and np.array_equal(x, y), f
+    envs, p, zs, zr, pr = B.prepare(*args, dict(kw))
+    b = B.build_batch(envs, p, zs, zr, pr, True)
+    assert b.envs["n_zss"].tolist() == [len(z) for z in args[3]]
+
+
+def test_padded_batch_errors_name_the_first_bad_ray():
+    # a NaN inside a profile's valid part leaves a gap that the loop reports
+    args, kw = _ragged_batch(20, 10)
+    args[5][11] = args[5][11].copy()
+    args[5][11][0, 0] = np.nan
+    norm = [B.normalize_to_batch(x, 20, "x") for x in args[3:]]
+    assert B.check_batch(20, np.asarray(args[1]), np.asarray(args[2]), *norm) is None
+    with pytest.raises(ValueError, match="Ray 11: cw contains non-finite"):
         B.prepare(*args, dict(kw))
