@@ -9,7 +9,8 @@ this class only normalises, validates and reshapes on the host.
 Extra keyword arguments (not in the reference):
 
 ``precision``  ``"plain"`` (complex128, default) or ``"chosen"`` (complex64
-               sweeps with an FP64-residual refinement step).
+               sweeps in FP32 arithmetic; the Pade terms are combined in FP64
+               and the field is kept in complex128).
 ``per_ray``    ``True`` pairs environment i with frequency i (no
                environment x frequency cross product) and gives every ray its
                own grid; ``zs``, ``zr``, ``dr``, ``dz``, ``np``, ``rmax`` may

@@ -45,8 +45,9 @@ enum cr_status {
 /* Arithmetic form of the range march. */
 enum cr_precision {
     CR_PLAIN_C128 = 0,   /* complex128 field and sweeps, FP64 arithmetic          */
-    CR_CHOSEN_C64R = 1   /* complex64 sweeps, FP32 accumulation, one FP64-residual
-                            refinement step per Pade term; field kept in complex128 */
+    CR_CHOSEN_C64R = 1   /* complex64 factors, workspace and sweeps (FP32 arithmetic);
+                            the Pade terms are combined in FP64 and the field is
+                            kept in complex128                                    */
 };
 
 /*

@@ -37,7 +37,7 @@
  *          formed in float32 and d1..d3 in complex64.  Used only to pin the
  *          oracle to the fixtures at rounding level.
  *
- * Parity pinned against: tests/golden/*.npz (the reference itself run on CPU
+ * Parity pinned against: the .npz fixtures of tests/golden (the reference itself run on CPU
  * under Numba's CUDA simulator) and RAM v1.5's tl_ref.line.
  */
 #include <complex.h>
