@@ -155,3 +155,49 @@ def test_surface_source_falls_back_to_product_form(cuda_device):
         out = eng.run()
     ref = oracle.run(b, "plain")
     assert np.abs(out["tll"][:b.line_len] - ref["tll"][:b.line_len]).max() < TOL_ORACLE
+
+
+def _mixed_batch(n_short=3500, idx=None):
+    """3500 short rays (nz 99, 59 steps) and two long ones (nz 299, 2999 steps),
+    per-ray grids: a ray's lockstep march alone (0.3 us per row and step)
+    exceeds 1.25x the batch's balanced time (work / 1.3e10 per s) only for the
+    long rays.  idx selects a subset of the same rays."""
+    long_ids = {0, n_short // 2 + 1}
+    is_long = [i in long_ids for i in range(n_short + 2)]
+    if idx is not None:
+        is_long = [is_long[i] for i in idx]
+    n = len(is_long)
+    rmax = np.array([30000.0 if L else 600.0 for L in is_long])
+    dep = [200.0 if L else 40.0 for L in is_long]
+    args = [np.full(n, 100.0), np.full(n, 10.0), np.full(n, 10.0),
+            [np.array([0.0, 250.0 if L else 60.0]) for L in is_long], [np.array([0.0])] * n,
+            [np.array([[1500.0], [1500.0]])] * n, [np.array([0.0, 20.0 if L else 10.0]) for L in is_long],
+            [np.array([0.0])] * n, [np.array([[1700.0], [1700.0]])] * n, [np.array([[1.5], [1.5]])] * n,
+            [np.array([[0.5], [0.5]])] * n, [np.array([[0.0, d], [r, d]]) for d, r in zip(dep, rmax)]]
+    kw = dict(batch_size=n, per_ray=True, dz=1.0, dr=10.0, rmax=rmax, np=4, lyrw=2)
+    envs, p, zs, zr, pr = B.prepare(*args, kw)
+    return B.build_batch(envs, p, zs, zr, pr, False), sorted(long_ids)
+
+
+def test_mixed_batch_column_and_batched_vs_oracle(cuda_device):
+    """The default policy splits this batch: the two long rays go to the column
+    kernel, the short ones stay on the batched kernel, and both launches run
+    concurrently.  The long rays and every 70th short ray are checked against
+    the oracle (rays are independent, so a sub-batch of the same rays serves)."""
+    b, longs = _mixed_batch()
+    with Engine(b) as eng:
+        out = eng.run()
+        st = eng.stats()
+    assert st["rays_failed"] == 0
+    assert st["column_rays"] == 2
+    idx = sorted(set(longs) | set(range(1, b.n_rays, 70)))
+    sub, _ = _mixed_batch(idx=idx)
+    ref = oracle.run(sub, "plain")
+    for j, i in enumerate(idx):
+        r, s = b.rays[i], sub.rays[j]
+        assert (int(r["nvr"]), int(r["nz"])) == (int(s["nvr"]), int(s["nz"]))
+        lo, so, n = int(r["line_off"]), int(s["line_off"]), int(r["nvr"])
+        d = np.abs(out["tll"][lo:lo + n] - ref["tll"][so:so + n]).max()
+        assert d < TOL_ORACLE, (i, d)
+        c = np.abs(out["cpl"][lo:lo + n] - ref["cpl"][so:so + n]).max() / np.abs(ref["cpl"][so:so + n]).max()
+        assert c < 1e-6, (i, c)
