@@ -123,6 +123,14 @@ def tc_error_flag():
     return _err
 
 
+def check_tc_flag():
+    """Raise if a tcgen05 GEMM gave up one of its bounded waits (its output is then
+    incomplete).  The flag is sticky: it is only ever cleared by the caller."""
+    if _err is not None and int(_err.item()) != 0:
+        raise RuntimeError("cr_mlp_gemm_tc: a bounded wait gave up (pipeline stalled); "
+                           "the GEMM results since the flag was last cleared are invalid")
+
+
 def gemm(epi, A, B, out, bias=None, mask=None, tc=None):
     """out = epilogue(A B^T); A [M, K], B [N, K] bf16 (K-contiguous rows).  tc: use the tcgen05 kernel
     (default: USE_TCGEN05 where N is a multiple of 256 and K of 64)."""
@@ -425,13 +433,16 @@ class Ensemble:
                     m.step(lr * 0.5 * (1.0 + math.cos(math.pi * frac)))
                     step += 1
                 mse = float(sse.item()) / (steps_per_epoch * batch * Y.shape[1])
+                check_tc_flag()
                 if log:
                     log(f"model {k} epoch {ep}: rms {math.sqrt(mse) * TL_SCALE:.2f} dB")
             losses.append(math.sqrt(mse) * TL_SCALE)
         return losses
 
-    def predict(self, X, chunk=8192):
-        """TL mean and spread over the members, [n, 64, 128] each (dB, float32 device tensors)."""
+    def predict(self, X, chunk=8192, check=True):
+        """TL mean and spread over the members, [n, 64, 128] each (dB, float32 device tensors).
+        check: synchronise and raise if a tensor-core GEMM gave up a wait (callers that
+        synchronise anyway pass False and call check_tc_flag themselves)."""
         import torch
         n = X.shape[0]
         mean = torch.empty(n, NZ_OUT * NR_OUT, device=X.device)
@@ -442,6 +453,8 @@ class Ensemble:
             preds.clamp_(TL_LO, TL_HI)
             mean[s: s + chunk] = preds.mean(0)
             spread[s: s + chunk] = preds.std(0, unbiased=False)
+        if check:
+            check_tc_flag()
         return mean.view(n, NZ_OUT, NR_OUT), spread.view(n, NZ_OUT, NR_OUT)
 
 
@@ -478,9 +491,10 @@ def serve(ens: Ensemble, q: Requests, threshold_db=1.0):
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
-    mean, spread = ens.predict(X)
+    mean, spread = ens.predict(X, check=False)
     e1.record()
     torch.cuda.synchronize()
+    check_tc_flag()
     t_net = e0.elapsed_time(e1) * 1e-3
     srms = torch.sqrt((spread[:n] ** 2).mean(dim=(1, 2))).cpu().numpy()
     tl = mean[:n].cpu().numpy()

@@ -36,7 +36,8 @@ enum cr_status {
     CR_EINVAL = 1,    /* invalid argument or inconsistent batch description */
     CR_ECUDA = 2,     /* CUDA runtime error (text in cr_last_error)          */
     CR_EPADE = 3,     /* Pade root finding did not converge                   */
-    CR_ETIMEOUT = 4,  /* a device-side iteration cap was hit                  */
+    CR_ETIMEOUT = 4,  /* a device-side iteration cap was hit (reserved: the
+                         march kernels have no waits of their own)            */
     CR_ENAN = 5,      /* a ray produced a non-finite field (see cr_ray_flags) */
     CR_ENOMEM = 6,    /* device or host allocation failed                     */
     CR_ESTATE = 7     /* call made in the wrong order (e.g. march before upload) */

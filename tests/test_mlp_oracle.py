@@ -1,5 +1,7 @@
-"""The MLP oracle itself (CPU): its backward pass against finite differences."""
+"""The MLP oracle itself (CPU): its backward pass against finite differences.
+Also the surrogate's host check of the tensor-core GEMM's wait flag."""
 import numpy as np
+import pytest
 
 from oracle import mlp_oracle as M
 
@@ -42,3 +44,17 @@ def test_bf16_rounding():
     assert r[0] == 1.0 and r[1] == 1.0  # halfway rounds to even
     assert r[2] == 1.0078125
     assert abs(r[3] + 3.140625) < 1e-12 and r[4] == 0.0
+
+
+def test_tensor_core_wait_flag_is_checked(monkeypatch):
+    """A set flag (a bounded wait of the tcgen05 GEMM gave up) makes training and
+    serving raise instead of returning the incomplete results."""
+    import torch
+    from cupyram_b200 import surrogate as S
+    monkeypatch.setattr(S, "_err", torch.zeros(1, dtype=torch.int32))
+    S.check_tc_flag()
+    S._err.fill_(1)
+    with pytest.raises(RuntimeError, match="bounded wait"):
+        S.check_tc_flag()
+    monkeypatch.setattr(S, "_err", None)
+    S.check_tc_flag()  # no GEMM has run: nothing to check
