@@ -13,7 +13,7 @@
 // then find the roots of the numerator and denominator polynomials by
 // Laguerre's method with deflation; pd = -1 / root.
 //
-// Behaviour follows the reference's cupyram/pade.py:160-417 (same constraint
+// Behaviour follows the reference's cupyram/pade.py:17-273 (same constraint
 // rows, the same Laguerre schedule: 1000-iteration search to 1e-12 then a
 // 5-iteration polish, a quarter-turn kick every 9 iterations, failure after
 // 100 iterations).

@@ -1,10 +1,10 @@
 """Pade coefficients (host FP64, native).
 
 ``compute_pade_coefficients`` keeps the signature and return values of the
-reference's ``cupyram/pade.py:324-417``: two complex128 arrays of length
+reference's ``cupyram/pade.py:180-273``: two complex128 arrays of length
 ``np_pade`` (product-form numerator and denominator coefficients).  A failed
 Laguerre iteration raises ``ValueError('Laguerre method not converging')``
-as the reference does (``pade.py:290-291``).
+as the reference does (``pade.py:146-147``).
 """
 import numpy as np
 

@@ -137,10 +137,10 @@ int cr_abi_version(void);
 /*
  * Pade coefficients of exp(i*k0*dr*(sqrt(1+X)-1)) (ip=1) or of the
  * self-starter operator (ip=2), product form, FP64.
- * Replaces cupyram/pade.py:324-417 compute_pade_coefficients(freq, c0,
+ * Replaces cupyram/pade.py:180-273 compute_pade_coefficients(freq, c0,
  * np_pade, ns, dr, ip).  pd1, pd2: 2*np doubles each (re, im interleaved).
  * Returns CR_EPADE when Laguerre iteration fails to converge
- * (cupyram/pade.py:290-291 raises ValueError there).
+ * (cupyram/pade.py:146-147 raises ValueError there).
  */
 int cr_pade(double freq, double c0, int np, int ns, double dr, int ip,
             double* pd1, double* pd2);

@@ -14,7 +14,7 @@
  *   outpt      cupyram/outpt.py:11-57
  *   selfs      cupyram/cupyram.py:1001-1063
  *   run loop   cupyram/cupyram.py:273-317
- *   epade      cupyram/pade.py:160-417
+ *   epade      cupyram/pade.py:17-273
  *
  * Modes (ORACLE_*):
  *   REF    storage rounded exactly where the reference rounds: f1..f3, cw, cb,
@@ -59,7 +59,7 @@
 typedef double complex cd;
 
 /* ------------------------------------------------------------------------- */
-/* Pade coefficients (cupyram/pade.py:160-417, RAM's epade)                   */
+/* Pade coefficients (cupyram/pade.py:17-273, RAM's epade)                   */
 /* ------------------------------------------------------------------------- */
 static cd cpow_int(cd z, int n) {
     cd r = 1.0;
@@ -67,7 +67,7 @@ static cd cpow_int(cd z, int n) {
     return r;
 }
 
-/* Laguerre iteration for one root of a[0..n] (pade.py:238-293).
+/* Laguerre iteration for one root of a[0..n] (pade.py:95-149).
    Returns 0 on success, -1 when 100 iterations pass without convergence. */
 static int guerre(cd* a, int n, cd* zio, double err, int nter) {
     cd az[2 * CR_MAX_NP + 2], azz[2 * CR_MAX_NP + 2];
@@ -102,7 +102,7 @@ static int guerre(cd* a, int n, cd* zio, double err, int nter) {
     return 0;
 }
 
-/* All roots of the degree-n polynomial a[0..n] (pade.py:296-321). */
+/* All roots of the degree-n polynomial a[0..n] (pade.py:153-177). */
 static int fndrt(cd* a, int n, cd* z) {
     if (n == 1) { z[0] = -a[0] / a[1]; return 0; }
     if (n != 2) {
@@ -146,7 +146,7 @@ int oracle_pade(double freq, double c0, int np, int ns, double dr, int ip, cd* p
     for (int i = 2; i <= n; ++i)
         for (int j = 1; j < i; ++j) bin[i][j] = bin[i - 1][j - 1] + bin[i - 1][j];
 
-    /* derivatives of the operator function at x=0 (pade.py:160-187) */
+    /* derivatives of the operator function at x=0 (pade.py:17-43) */
     dh1[0] = 0.5 * I * sig;
     double exp1 = -0.5;
     dh2[0] = alp;
@@ -164,14 +164,14 @@ int oracle_pade(double freq, double c0, int np, int ns, double dr, int ip, cd* p
         dg[i + 1] = dh1[i] + dh2[i] + dh3[i];
         for (int j = 0; j < i; ++j) dg[i + 1] += bin[i][j] * (dh1[j] + dh2[j] + dh3[j]) * dg[i - j];
     }
-    /* accuracy constraints (pade.py:373-382) */
+    /* accuracy constraints (pade.py:229-238) */
     for (int i = 0; i < n; ++i) b[i] = dg[i + 1];
     for (int i = 0; i < n; ++i) {
         if (2 * i <= n - 1) a[i][2 * i] = fact[i];
         for (int j = 0; j <= i; ++j)
             if (2 * j + 1 <= n - 1) a[i][2 * j + 1] = -bin[i + 1][j + 1] * fact[j] * dg[i - j];
     }
-    /* stability constraints (pade.py:384-397) */
+    /* stability constraints (pade.py:240-256) */
     if (ns >= 1) {
         cd z1 = -3.0;
         b[n - 1] = -1.0;
@@ -182,7 +182,7 @@ int oracle_pade(double freq, double c0, int np, int ns, double dr, int ip, cd* p
         b[n - 2] = -1.0;
         for (int j = 0; j < np; ++j) { a[n - 2][2 * j] = cpow_int(z1, j + 1); a[n - 2][2 * j + 1] = 0.0; }
     }
-    /* Gaussian elimination with partial pivoting (pade.py:190-235) */
+    /* Gaussian elimination with partial pivoting (pade.py:47-91) */
     for (int i = 0; i < n; ++i) {
         if (i < n - 1) {
             int i0 = i;
