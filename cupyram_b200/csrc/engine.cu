@@ -905,9 +905,12 @@ std::vector<int> column_clusters(const cr_batch* b, const std::vector<int>& pd_n
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const int share = std::max(1, sms / n_col);
-    std::map<std::tuple<int, int, int>, bool> runs, dense;
-    const char* env2 = getenv("CUPYRAM_B200_COL2");  // "0": keep the smallest cluster
-    const bool two_per_sm = !(env2 && env2[0] == '0');
+    std::map<std::tuple<int, int, int>, bool> runs;
+    std::map<std::tuple<int, int, int>, int> dense;  // resident CTAs of a cluster size
+    // target CTAs per SM for throughput-bound column launches ("0": keep the
+    // smallest cluster)
+    const char* env2 = getenv("CUPYRAM_B200_COL2");
+    const int per_sm = env2 ? std::max(0, std::min(4, env2[0] - '0')) : 3;
     for (int i = 0; i < b->n_rays; ++i) {
         if (!is_col[(size_t)i]) continue;
         const int nz = b->rays[i].nz, terms = col_terms(pd_n, i);
@@ -920,17 +923,20 @@ std::vector<int> column_clusters(const cr_batch* b, const std::vector<int>& pd_n
             if (it->second) break;
         }
         // many column rays: the launches are throughput-bound.  A larger
-        // cluster whose CTAs fit two to an SM doubles the warps that hide
-        // each other's latencies.
-        if (two_per_sm && (long long)n_col * cmin > sms) {
-            for (int C2 = C + 1; C2 <= 16; ++C2) {
-                const auto key = std::make_tuple(C2, terms, nz);
-                auto it = dense.find(key);
-                if (it == dense.end())
-                    it = dense.emplace(key, (long long)crk::col_max_active_clusters(C2, terms, nz, chosen) * C2 >=
-                                                3LL * sms / 2).first;
-                if (it->second) {
-                    C = C2;
+        // cluster whose CTAs fit three (else two) to an SM multiplies the
+        // warps that hide each other's latencies.
+        if (per_sm > 1 && (long long)n_col * cmin > sms) {
+            for (int want = per_sm; want >= 2; --want) {
+                int found = 0;
+                for (int C2 = C + 1; C2 <= 16 && !found; ++C2) {
+                    const auto key = std::make_tuple(C2, terms, nz);
+                    auto it = dense.find(key);
+                    if (it == dense.end())
+                        it = dense.emplace(key, crk::col_max_active_clusters(C2, terms, nz, chosen) * C2).first;
+                    if (2LL * it->second >= (2LL * want - 1) * sms) found = C2;
+                }
+                if (found) {
+                    C = found;
                     break;
                 }
             }
