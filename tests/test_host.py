@@ -211,3 +211,47 @@ def test_padded_batch_errors_name_the_first_bad_ray():
     assert B.check_batch(20, np.asarray(args[1]), np.asarray(args[2]), *norm) is None
     with pytest.raises(ValueError, match="Ray 11: cw contains non-finite"):
         B.prepare(*args, dict(kw))
+
+
+@pytest.mark.parametrize("kw,match", [
+    (dict(np=0), "np must be"), (dict(np=11), "np must be"), (dict(dr=-1.0), "dr and dz"), (dict(dz=0.0), "dr and dz"),
+    (dict(ns=3), "ns must be"), (dict(ndr=0), "ndr and ndz"), (dict(ndz=0), "ndr and ndz"),
+    (dict(batch_size=0), "batch_size"), (dict(rmax=1.0, dr=50.0), "rmax must cover"),
+])
+def test_invalid_parameters_raise(kw, match):
+    with pytest.raises(ValueError, match=match):
+        envs, p, zs, zr, pr = prep(pekeris(), **kw)
+        B.build_batch(envs, p, zs, zr, pr, False)
+
+
+@pytest.mark.parametrize("freq", [0.0, -50.0, float("nan"), []])
+def test_invalid_frequency_raises(freq):
+    with pytest.raises(ValueError, match="freq"):
+        prep(pekeris(freq=freq))
+
+
+def test_per_ray_values_must_match_the_batch():
+    d = pekeris(z_ss=[np.array([0.0, 200.0])] * 2, rp_ss=[np.array([0.0])] * 2,
+                cw=[np.array([[1500.0], [1500.0]])] * 2, z_sb=[np.array([0.0])] * 2, rp_sb=[np.array([0.0])] * 2,
+                cb=[np.array([[1700.0]])] * 2, rhob=[np.array([[1.5]])] * 2, attn=[np.array([[0.5]])] * 2,
+                rbzb=[np.array([[0.0, 200.0], [5000.0, 200.0]])] * 2)
+    with pytest.raises(ValueError, match="zs"):
+        B.prepare(*[dict(d, zs=[100.0, 90.0, 80.0])[k] for k in ORDER], dict(batch_size=2, per_ray=True))
+    with pytest.raises(ValueError, match="scalars unless per_ray"):
+        B.prepare(*[dict(d, zs=[100.0, 90.0])[k] for k in ORDER], dict(batch_size=2))
+    with pytest.raises(ValueError, match="list length"):
+        B.prepare(*[d[k] for k in ORDER], dict(batch_size=3))
+    # per-ray np, dr and output decimation are taken ray by ray
+    envs, p, zs, zr, pr = B.prepare(*[dict(d, freq=[50.0, 100.0])[k] for k in ORDER],
+                                    dict(batch_size=2, per_ray=True, np=np.array([4, 8]), ndr=np.array([1, 2]),
+                                         ndz=np.array([2, 3])))
+    b = B.build_batch(envs, p, zs, zr, pr, True)
+    assert b.rays["np"].tolist() == [4, 8] and b.rays["ndr"].tolist() == [1, 2] and b.rays["ndz"].tolist() == [2, 3]
+    assert b.rays["dr"].tolist() == [4 * 1500.0 / 50.0, 8 * 1500.0 / 100.0]  # dr = np c / f per ray
+
+
+def test_c0_override_and_default():
+    envs, p, *_ = prep(pekeris(cw=np.array([[1490.0], [1510.0]])), rmax=1000.0)
+    assert p.c0_env[0] == pytest.approx(1500.0)  # mean of the first water profile
+    envs, p, *_ = prep(pekeris(), rmax=1000.0, c0=1480.0)
+    assert p.c0_env[0] == 1480.0 and p.c0_report == 1480.0
