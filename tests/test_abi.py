@@ -62,6 +62,19 @@ def test_pade_matches_reference(lib_built):
     assert worst < 1e-8, worst
 
 
+def test_pade_batch_matches_single_calls(lib_built):
+    """compute_pade_coefficients_batch (cupyram/pade.py:276-317): [np, batch]
+    arrays whose column b is the single call at c0_array[b]."""
+    from cupyram_b200 import compute_pade_coefficients, compute_pade_coefficients_batch
+    c0 = np.array([1480.0, 1500.0, 1525.0, 1550.0])
+    for npd, ns, ip in ((4, 1, 1), (6, 2, 1), (8, 1, 2)):
+        pd1, pd2 = compute_pade_coefficients_batch(75.0, c0, npd, ns, 20.0, ip)
+        assert pd1.shape == pd2.shape == (npd, c0.size) and pd1.dtype == np.complex128
+        for b, c in enumerate(c0):
+            q1, q2 = compute_pade_coefficients(75.0, c, npd, ns=ns, dr=20.0, ip=ip)
+            assert np.array_equal(pd1[:, b], q1) and np.array_equal(pd2[:, b], q2)
+
+
 def test_pade_bad_arguments(lib_built):
     with pytest.raises(ValueError):
         compute_pade_coefficients(50.0, 1500.0, 0)
