@@ -32,6 +32,7 @@
 //   receiver / TL grid      cupyram/outpt.py:11-57
 //   self-starter            cupyram/cupyram.py:1001-1063
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <atomic>
@@ -796,6 +797,17 @@ int compute_pade_sets(cr_engine* e, const cr_batch* b) {
 
 }  // namespace
 
+namespace {
+// Named NVTX range over an entry point, for timelines in profilers (no cost
+// when no tool is attached).
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
+}  // namespace
+
 extern "C" {
 
 int cr_abi_version(void) { return CR_ABI_VERSION; }
@@ -1009,6 +1021,7 @@ std::vector<char> pick_column_rays(const cr_batch* b, const std::vector<int>& pd
 }  // namespace
 
 int cr_create(const cr_batch* b, cr_engine** out) {
+    NvtxRange nv("cr_create");
     if (!out) {
         set_global_error("cr_create: out is NULL");
         return CR_EINVAL;
@@ -1334,6 +1347,7 @@ int cr_set_pade(cr_engine* e, int ray, int which, int n, const double* pd1, cons
 }
 
 int cr_upload(cr_engine* e) {
+    NvtxRange nv("cr_upload");
     if (!e) return CR_EINVAL;
     cudaError_t ce = cudaSetDevice(e->device);
     float ms = 0.f;
@@ -1369,6 +1383,7 @@ int cr_upload(cr_engine* e) {
 }
 
 int cr_march(cr_engine* e) {
+    NvtxRange nv("cr_march");
     if (!e) return CR_EINVAL;
     if (!e->uploaded) return e->fail(CR_ESTATE, "cr_march: call cr_upload first");
     cudaError_t ce = cudaSetDevice(e->device);
@@ -1504,6 +1519,7 @@ int cr_march(cr_engine* e) {
 }
 
 int cr_download(cr_engine* e, const cr_outputs* out) {
+    NvtxRange nv("cr_download");
     if (!e) return CR_EINVAL;
     if (!out || !out->tll || !out->cpl) return e->fail(CR_EINVAL, "cr_download: tll and cpl are required");
     if (!e->marched) return e->fail(CR_ESTATE, "cr_download: nothing marched yet");
@@ -1567,6 +1583,7 @@ __global__ void cell_tl_kernel(const RayDev* __restrict__ rays, int n_rays, cons
 }  // namespace
 
 int cr_cell_tl(cr_engine* e, int sz, int sr, int ncz, int ncr, float* tl_cells) {
+    NvtxRange nv("cr_cell_tl");
     if (!e) return CR_EINVAL;
     if (sz < 1 || sr < 1 || ncz < 1 || ncr < 1 || !tl_cells) return e->fail(CR_EINVAL, "cr_cell_tl: invalid arguments");
     if (!e->compute_grids) return e->fail(CR_EINVAL, "cr_cell_tl: the batch computes no TL grid");
@@ -1784,6 +1801,7 @@ __global__ void static_flags_kernel(const int* flags, int n, int* status) {
 }  // namespace
 
 extern "C" int cr_march_static(const cr_batch* b, const cr_outputs* out, void* stream_v) {
+    NvtxRange nv("cr_march_static");
     const std::string msg = [&]() -> std::string {
         if (!out || !out->tll || !out->cpl) return "dev_out with tll and cpl device pointers is required";
         return std::string();
