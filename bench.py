@@ -183,24 +183,33 @@ class ClockSampler:
                 self.p.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.p.kill()
+        self.f.close()
+        path = Path(self.f.name)
+        self._summary = parse_clocks(path.read_text())
+        path.unlink(missing_ok=True)
 
     def summary(self):
-        self.f.flush()
-        rows = []
-        for line in Path(self.f.name).read_text().splitlines():
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
-            except ValueError:
-                continue
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
-        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": rows[0][1],
-                "reasons": reasons, "samples": len(rows)}
+        return self._summary
+
+
+def parse_clocks(text):
+    """Median SM clock, max clock and active throttle reasons from nvidia-smi
+    CSV rows (no header, no units) of ClockSampler.Q."""
+    rows = []
+    for line in text.splitlines():
+        parts = [x.strip() for x in line.split(",")]
+        if len(parts) < 9:
+            continue
+        try:
+            rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+        except ValueError:
+            continue
+    if not rows:
+        return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+    return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": rows[0][1],
+            "reasons": reasons, "samples": len(rows)}
 
 
 def measured_peak_hbm():

@@ -1,0 +1,40 @@
+"""Host helpers of bench.py (CPU): the nvidia-smi clock record and the whole-job rate."""
+import os
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+sys.path.insert(0, str(Path(__file__).resolve().parent.parent))
+import bench  # noqa: E402
+
+ROWS = """0, 1965, 1965, 812.5, 0x0000000000000004, Not Active, Not Active, Not Active, Active
+0, 1702, 1965, 998.1, 0x0000000000000004, Not Active, Not Active, Not Active, Active
+0, 1507, 1965, 1001.0, 0x0000000000000004, Not Active, Not Active, Not Active, Active
+garbage line
+0, [N/A], 1965, 1.0, 0x0, Not Active, Not Active, Not Active, Not Active
+"""
+
+
+def test_clock_record_median_and_reasons():
+    c = bench.parse_clocks(ROWS)
+    assert c["samples"] == 3 and c["sm_mhz"] == 1702.0 and c["sm_max_mhz"] == 1965.0
+    assert c["reasons"] == ["sw_power_cap"]
+    hot = ROWS.replace("Not Active, Not Active, Not Active, Active", "Active, Not Active, Active, Not Active", 1)
+    assert bench.parse_clocks(hot)["reasons"] == ["hw_slowdown", "sw_power_cap", "sw_thermal_slowdown"]
+    assert bench.parse_clocks("")["reasons"] == ["unavailable"]
+
+
+def test_clock_sampler_without_a_gpu_leaves_no_file(monkeypatch):
+    monkeypatch.setenv("PATH", "/nonexistent")  # nvidia-smi cannot start
+    with bench.ClockSampler(0) as clk:
+        path = clk.f.name
+        assert os.path.exists(path)
+    assert not os.path.exists(path)
+    assert clk.summary() == {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+
+
+def test_whole_job_rate():
+    # updates of every rank over the slowest rank's time for the given steps
+    assert np.isclose(bench.whole_job_rate(4.0e10, 3, 6000.0), 4.0e10 * 3 / 6.0)
