@@ -116,3 +116,16 @@ def test_null_arguments(lib_built):
     assert lib.cr_upload(None) == _lib.CR_EINVAL
     assert lib.cr_march(None) == _lib.CR_EINVAL
     lib.cr_destroy(None)
+
+
+def test_header_constants_match_the_binding():
+    """The host binding's copies of the header's #defines and enums."""
+    text = (Path(__file__).resolve().parent.parent / "include" / "cupyram_b200.h").read_text()
+    defines = {k: v.replace("u", "") for k, v in re.findall(r"#define\s+(CR_\w+)\s+\(?([0-9][0-9u *]*)\)?", text)}
+    assert int(defines["CR_ABI_VERSION"]) == _lib.ABI_VERSION
+    assert int(defines["CR_MAX_NP"]) == _lib.MAX_NP
+    assert int(np.prod([int(x) for x in defines["CR_STATIC_SCRATCH_BYTES"].split("*")])) == _lib.STATIC_SCRATCH_BYTES
+    enums = {k: int(v) for k, v in re.findall(r"\b(CR_[A-Z0-9_]+)\s*=\s*(\d+)", text)}
+    for name in ("CR_OK", "CR_EINVAL", "CR_ECUDA", "CR_EPADE", "CR_ETIMEOUT", "CR_ENAN", "CR_ENOMEM", "CR_ESTATE",
+                 "CR_PLAIN_C128", "CR_CHOSEN_C64R"):
+        assert enums[name] == getattr(_lib, name), name
