@@ -31,6 +31,15 @@
  *          i.e. u_new = c_inf u + sum_k c_k (M + pd2_k D)^{-1} M u.  Same
  *          rational operator as the product form; used to check the engine's
  *          sum-form march against the product form.
+ *   CHOSEN, CHOSEN_C32, CHOSEN_F32
+ *          models of the engine's chosen form in sum form, rounded where
+ *          the batched kernel rounds: 1/den, w and the elimination's
+ *          coupling in complex64 (the factorisation recurrence itself in
+ *          FP64), M u rounded to complex64, the elimination and the
+ *          back-substitution in FP32.  CHOSEN combines the terms in FP64
+ *          (the engine's form); CHOSEN_C32 combines them in FP32; CHOSEN_F32
+ *          also forms the coupling in FP32 from a complex64 d1.  Used by
+ *          oracle/chosen_study.py to size the error of an FP32 inner loop.
  *   SIM    REF plus the scalar promotions of Numba's CUDA simulator under
  *          NumPy 2 (a Python float times a float32 stays float32), which is
  *          how the golden fixtures were produced: the Galerkin c1..c3 are
@@ -55,6 +64,9 @@
 #define ORACLE_F64 2
 #define ORACLE_SIM 3
 #define ORACLE_SUM 4
+#define ORACLE_CHOSEN 5
+#define ORACLE_CHOSEN_C32 6
+#define ORACLE_CHOSEN_F32 7
 
 typedef double complex cd;
 
@@ -468,6 +480,78 @@ static void march_step_sum(ray_state* s, int n, const cd* pd1, const cd* pd2) {
     free(x);
 }
 
+typedef float complex cf;
+static inline cf to_c64(cd z) { return (float)creal(z) + I * (float)cimag(z); }
+static inline cd to_c128(cf z) { return (double)crealf(z) + I * (double)cimagf(z); }
+
+/* One range step of the chosen-form models (see ORACLE_CHOSEN): sum form,
+   downward elimination, complex64 factors and FP32 recurrences.  comb32:
+   terms combined in FP32; coupling32: the coupling -(a1 + pd2 d1)/den
+   formed in FP32 from a complex64 d1. */
+static void march_step_chosen(ray_state* s, int n, const cd* pd1, const cd* pd2, int comb32, int coupling32) {
+    const int nz = s->nz;
+    cd cinf = 1.0;
+    for (int j = 0; j < n; ++j) cinf *= pd1[j] / pd2[j];
+    cf* mu = (cf*)malloc(sizeof(cf) * (size_t)(nz + 2));
+    cd* acc = (cd*)malloc(sizeof(cd) * (size_t)(nz + 2));
+    cf* accf = (cf*)malloc(sizeof(cf) * (size_t)(nz + 2));
+    cf* g = (cf*)malloc(sizeof(cf) * (size_t)(nz + 2));
+    cf* x = (cf*)malloc(sizeof(cf) * (size_t)(nz + 2));
+    cf* q = (cf*)malloc(sizeof(cf) * (size_t)(nz + 2));
+    cf* w = (cf*)malloc(sizeof(cf) * (size_t)(nz + 2));
+    cf* al = (cf*)malloc(sizeof(cf) * (size_t)(nz + 2));
+    const double a1 = s->k0 * s->k0 / 6.0, a2 = 2.0 * s->k0 * s->k0 / 3.0;
+    for (int i = 1; i <= nz; ++i) {
+        mu[i] = to_c64(a1 * (s->u[i - 1] + s->u[i + 1]) + a2 * s->u[i]);
+        acc[i] = cinf * s->u[i];
+        accf[i] = to_c64(cinf) * to_c64(s->u[i]);
+    }
+    for (int k = 0; k < n; ++k) {
+        cd ck = 1.0 - pd1[k] / pd2[k];
+        for (int j = 0; j < n; ++j)
+            if (j != k) ck *= (1.0 - pd1[j] / pd2[k]) / (1.0 - pd2[j] / pd2[k]);
+        const cd zero = 0.0;
+        cd r[3], rq[3];
+        cd wp = 0.0;
+        for (int i = 1; i <= nz; ++i) {
+            galerkin(s, i, zero, pd2[k], r, rq);
+            const cd qd = 1.0 / (r[1] - r[0] * wp);
+            wp = r[2] * qd;
+            q[i] = to_c64(qd);
+            w[i] = to_c64(wp);
+            if (coupling32) {
+                cd r1[3], q1[3];
+                galerkin(s, i, zero, 1.0, r1, q1);  /* a1 + d1 */
+                const cf cin = (float)a1 + to_c64(pd2[k]) * to_c64(r1[0] - a1);
+                al[i] = -(cin * q[i]);
+            } else {
+                al[i] = to_c64(-(r[0] * to_c128(q[i])));
+            }
+        }
+        cf gp = 0.0f;
+        for (int i = 1; i <= nz; ++i) {
+            gp = q[i] * mu[i] + al[i] * gp;
+            g[i] = gp;
+        }
+        x[nz] = g[nz];
+        for (int i = nz - 1; i >= 1; --i) x[i] = g[i] - w[i] * x[i + 1];
+        const cf ckf = to_c64(ck);
+        for (int i = 1; i <= nz; ++i) {
+            acc[i] += ck * to_c128(x[i]);
+            accf[i] += ckf * x[i];
+        }
+    }
+    for (int i = 1; i <= nz; ++i) s->u[i] = comb32 ? to_c128(accf[i]) : acc[i];
+    free(mu);
+    free(acc);
+    free(accf);
+    free(g);
+    free(x);
+    free(q);
+    free(w);
+    free(al);
+}
+
 /* updat (updat.py:38-140): returns 1 when the profiles must be re-interpolated. */
 static int updat(ray_state* s, double r) {
     int need = 0;
@@ -607,7 +691,13 @@ static int run_ray(const cr_batch* b, int ib, int mode, double* tll_all, double*
     for (int j = 0; j < CR_MAX_NP; ++j) { pd1[j] = 0.0; pd2[j] = 0.0; }
     pd2[0] = -1.0;
     const int nself = (mode == ORACLE_REF || mode == ORACLE_SIM) ? np : 1;
-    if (mode == ORACLE_SUM) {
+    const int chosen = mode == ORACLE_CHOSEN || mode == ORACLE_CHOSEN_C32 || mode == ORACLE_CHOSEN_F32;
+    const int comb32 = mode == ORACLE_CHOSEN_C32 || mode == ORACLE_CHOSEN_F32, coupling32 = mode == ORACLE_CHOSEN_F32;
+    if (chosen) {
+        march_step_chosen(&s, 1, pd1, pd2, comb32, coupling32);
+        march_step_chosen(&s, 1, pd1, pd2, comb32, coupling32);
+        march_step_chosen(&s, np, sp1, sp2, comb32, coupling32);
+    } else if (mode == ORACLE_SUM) {
         march_step_sum(&s, 1, pd1, pd2);
         march_step_sum(&s, 1, pd1, pd2);
         march_step_sum(&s, np, sp1, sp2);
@@ -630,7 +720,8 @@ static int run_ray(const cr_batch* b, int ib, int mode, double* tll_all, double*
             rs_lim = INFINITY;
         }
         init_profiles(&s);
-        if (mode == ORACLE_SUM) march_step_sum(&s, np, mp1, mp2);
+        if (chosen) march_step_chosen(&s, np, mp1, mp2, comb32, coupling32);
+        else if (mode == ORACLE_SUM) march_step_sum(&s, np, mp1, mp2);
         else march_step(&s, np, mp1, mp2);
         r = (double)(rn + 2) * s.dr;
         outpt(&s, ry, r, &mdr, &tlc, tll, cpl, tlg, cpg);

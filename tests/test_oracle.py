@@ -104,3 +104,17 @@ def test_oracle_batch_rays_independent():
         lo, n = int(b.rays["line_off"][k]), int(b.rays["nvr"][k])
         # the single-ray run starts its line at the ray's own offset
         assert np.array_equal(one["tll"][lo:lo + n], full["tll"][lo:lo + n])
+
+
+@pytest.mark.parametrize("name", ["mini_munk", "wedge_switch", "pekeris_small"])
+def test_chosen_form_models(name):
+    """The oracle's chosen-form models (complex64 sweeps; FP64 or FP32 term
+    combination; FP64 or FP32 coupling) round, and on these short cases stay
+    within 0.01 dB RMS of the FP64 sum form over cells with TL < 100 dB.
+    oracle/chosen_study.py runs them at the benchmark workloads' full ranges."""
+    b, _ = _prep(name, False)
+    ref = oracle.run(b, "sum")["tll"][: b.line_len]
+    lit = ref < 100.0
+    for mode in ("chosen", "chosen_c32", "chosen_f32"):
+        d = (oracle.run(b, mode)["tll"][: b.line_len] - ref)[lit]
+        assert 1e-7 < np.abs(d).max() and np.sqrt(np.mean(d * d)) < 0.01, (mode, np.abs(d).max())
