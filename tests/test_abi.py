@@ -129,3 +129,19 @@ def test_header_constants_match_the_binding():
     for name in ("CR_OK", "CR_EINVAL", "CR_ECUDA", "CR_EPADE", "CR_ETIMEOUT", "CR_ENAN", "CR_ENOMEM", "CR_ESTATE",
                  "CR_PLAIN_C128", "CR_CHOSEN_C64R"):
         assert enums[name] == getattr(_lib, name), name
+
+
+def test_create_without_a_device_fails_cleanly(lib_built):
+    """A valid batch on a machine without a usable GPU: cr_create returns
+    CR_ECUDA with the runtime's message, the binding raises, and the process
+    carries on (the library never aborts)."""
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    from cupyram_b200.engine import Engine
+    from cupyram_b200._lib import EngineError
+    args, kw, _ = load_case("pekeris_small")
+    envs, p, zs, zr, pr = B.prepare(*args, dict(kw))
+    b = B.build_batch(envs, p, zs, zr, pr, False)
+    with pytest.raises(EngineError, match=r"status 2\].*cr_create"):
+        Engine(b)
