@@ -36,7 +36,9 @@ Other configurations (--config):
               per second of serving
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--form plain|chosen]
-                       [--config munk|pekeris|wedge|precision]
+                       [--config munk|pekeris|wedge|precision|surrogate|gemm]
+                       [--rays N] [--rmax M] [--seed S] [--no-chosen] [--no-cpu-baseline]
+       python bench.py --config surrogate [--train N] [--infer N] [--epochs E]
        python bench.py --impl reference ...   (CPU restatement on host cores)
 Multi-GPU: launch with torch.distributed.run; every rank marches its own
 seeded batch of the same size (weak scaling, no collective on the data path).
