@@ -36,7 +36,7 @@ Other configurations (--config):
               per second of serving
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--form plain|chosen]
-                       [--config munk|pekeris|wedge|precision|surrogate|gemm]
+                       [--config munk|pekeris|wedge|precision|surrogate|gemm|peaks]
                        [--rays N] [--rmax M] [--seed S] [--no-chosen] [--no-cpu-baseline]
        python bench.py --config surrogate [--train N] [--infer N] [--epochs E]
        python bench.py --impl reference ...   (CPU restatement on host cores)
@@ -69,7 +69,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--form", choices=["plain", "chosen"], default="plain")
-    ap.add_argument("--config", choices=["munk", "pekeris", "wedge", "precision", "surrogate", "gemm"], default="munk")
+    ap.add_argument("--config", choices=["munk", "pekeris", "wedge", "precision", "surrogate", "gemm", "peaks"],
+                    default="munk")
     ap.add_argument("--train", type=int, default=200_000, help="surrogate: training marches")
     ap.add_argument("--infer", type=int, default=65_536, help="surrogate: served requests")
     ap.add_argument("--epochs", type=int, default=60, help="surrogate: training epochs per member")
@@ -368,6 +369,35 @@ def measured_peak_bf16():
     return 1590.0, "fallback"
 
 
+def run_peaks(a, iters=1 << 16):
+    """FP64 and FP32 FMA throughput of the device (cr_peak_fma): the ALU roofline
+    beside the HBM one.  Best of `steps` timed launches after the warm-up."""
+    import ctypes
+    import torch
+    from cupyram_b200 import _lib
+    torch.cuda.set_device(0)
+    lib = _lib.load()
+    res = {}
+    with ClockSampler(0) as clk:
+        for name, fp64 in (("fp64", 1), ("fp32", 0)):
+            best = 0.0
+            for _ in range(max(1, a.steps)):
+                t, ms = ctypes.c_double(), ctypes.c_double()
+                rc = lib.cr_peak_fma(fp64, iters, ctypes.byref(t), ctypes.byref(ms))
+                if rc:
+                    raise RuntimeError(f"cr_peak_fma failed with status {rc}")
+                best = max(best, t.value)
+            res[name] = best
+    line = {"metric": "FMA throughput (2 flops per FMA)", "value": res["fp64"], "unit": "TFLOP/s", "n_gpus": 1,
+            "steps": a.steps, "warmup": 1, "higher_is_better": True, "dtype": "f64",
+            "data": "synthetic (register-only FMA chains)",
+            "config": {"workload": f"8 FMA chains per thread x {iters} iterations, 8 CTAs of 256 threads per SM",
+                       "config": "peaks"},
+            "fp64_tflops": res["fp64"], "fp32_tflops": res["fp32"], "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_gemm(a):
     """The surrogate's contraction on its inference shape (8192 x 8192 x 512, the last layer of a batch of
     8192 requests), tcgen05 and mma.sync kernels, TFLOP/s against the measured bf16 peak."""
@@ -419,6 +449,8 @@ def main():
         return run_surrogate(a)
     if a.config == "gemm":
         return run_gemm(a)
+    if a.config == "peaks":
+        return run_peaks(a)
     if a.impl == "reference":
         return run_reference(a)
     rank, world, local = dist_env()

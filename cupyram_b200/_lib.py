@@ -72,6 +72,8 @@ _SIGS = {
     "cr_get_stats": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(CrStats)]),
     "cr_last_error": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t]),
     "cr_global_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
+    "cr_peak_fma": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                   ctypes.POINTER(ctypes.c_double)]),
     "cr_destroy": (None, [ctypes.c_void_p]),
     "cr_march_static": (ctypes.c_int, [ctypes.POINTER(CrBatch), ctypes.POINTER(CrOutputs), ctypes.c_void_p]),
     "cr_cell_tl": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,

@@ -145,3 +145,15 @@ def test_create_without_a_device_fails_cleanly(lib_built):
     b = B.build_batch(envs, p, zs, zr, pr, False)
     with pytest.raises(EngineError, match=r"status 2\].*cr_create"):
         Engine(b)
+
+
+def test_peak_fma_arguments_and_no_device(lib_built):
+    """cr_peak_fma (include/cupyram_b200_peaks.h) rejects bad arguments before
+    any CUDA call, and without a usable GPU returns its CUDA status."""
+    lib = _lib.load()
+    t, ms = ctypes.c_double(), ctypes.c_double()
+    assert lib.cr_peak_fma(1, 0, ctypes.byref(t), ctypes.byref(ms)) == 1
+    assert lib.cr_peak_fma(1, 16, None, ctypes.byref(ms)) == 1
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        assert lib.cr_peak_fma(1, 16, ctypes.byref(t), ctypes.byref(ms)) == 2
