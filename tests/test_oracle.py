@@ -118,3 +118,24 @@ def test_chosen_form_models(name):
     for mode in ("chosen", "chosen_c32", "chosen_f32"):
         d = (oracle.run(b, mode)["tll"][: b.line_len] - ref)[lit]
         assert 1e-7 < np.abs(d).max() and np.sqrt(np.mean(d * d)) < 0.01, (mode, np.abs(d).max())
+
+
+def test_chosen_form_models_at_full_range():
+    """Two full-range rays of the 4096-ray Munk batch (1999 steps, nz ~ 5600):
+    the chosen-form model stays within 0.01 dB RMS of the FP64 sum form, and
+    the all-FP32 inner loop within the chosen form's 0.1 dB RMS bar (cells with
+    TL < 100 dB); oracle/chosen_study.py gives the full table."""
+    from cupyram_b200 import workloads
+    b = workloads.build(*workloads.munk_batch(4096, seed=2024), compute_grids=False)
+    rays = [0, 2048]
+    r = b.rays[rays]
+
+    def lines(mode):
+        out = oracle.run(b, mode, rays=rays)["tll"]
+        return [out[int(x["line_off"]): int(x["line_off"]) + int(x["nvr"])] for x in r]
+
+    ref = lines("sum")
+    for mode, bar in (("chosen", 0.01), ("chosen_f32", 0.1)):
+        for a, c in zip(ref, lines(mode)):
+            d = (c - a)[a < 100.0]
+            assert np.sqrt(np.mean(d * d)) < bar, (mode, np.sqrt(np.mean(d * d)))
