@@ -38,3 +38,20 @@ def test_clock_sampler_without_a_gpu_leaves_no_file(monkeypatch):
 def test_whole_job_rate():
     # updates of every rank over the slowest rank's time for the given steps
     assert np.isclose(bench.whole_job_rate(4.0e10, 3, 6000.0), 4.0e10 * 3 / 6.0)
+
+
+def test_clock_sampler_reads_a_running_sampler(tmp_path, monkeypatch):
+    """The sampling path as on a GPU box: a stand-in nvidia-smi that prints a
+    CSV row every 20 ms until it is terminated."""
+    import time
+    fake = tmp_path / "nvidia-smi"
+    fake.write_text("#!/bin/sh\nwhile true; do echo '0, 1800, 1965, 900.0, 0x4, Not Active, Not Active, "
+                    "Not Active, Active'; sleep 0.02; done\n")
+    fake.chmod(0o755)
+    monkeypatch.setenv("PATH", f"{tmp_path}:{os.environ.get('PATH', '')}")
+    with bench.ClockSampler(0) as clk:
+        path = clk.f.name
+        time.sleep(0.3)
+    c = clk.summary()
+    assert c["samples"] >= 3 and c["sm_mhz"] == 1800.0 and c["reasons"] == ["sw_power_cap"]
+    assert not os.path.exists(path)
