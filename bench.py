@@ -13,9 +13,12 @@ excluded).
 
 value : device time of the march (CUDA events on the engine's stream), inputs
         already resident in HBM.
-e2e   : the same march through the C ABI call cr_run with host buffers: H2D of
-        the batch's inputs, the march, D2H of the TL / CP lines into pinned host
-        memory, every step; host wall clock around the call.
+e2e   : the same march through the C ABI calls a user makes for a batch, with
+        host buffers, every step: cr_create (validation, device Pade sets,
+        tiling, device memory from the engine pool), cr_run (H2D of the batch's
+        inputs, the march, D2H of the TL / CP lines into pinned host memory)
+        and cr_destroy; host wall clock around the calls.  e2e_resident: cr_run
+        alone on an engine created beforehand.
 
 Other configurations (--config):
   pekeris   - Pekeris waveguide, one ray: 50 Hz, zs = zr = 50 m, 100 m water
@@ -35,7 +38,7 @@ Other configurations (--config):
               value = march grid-point updates the served requests stand for
               per second of serving
 
-Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--form plain|chosen]
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--form plain|chosen|fast]
                        [--config munk|pekeris|wedge|precision|surrogate|gemm|peaks]
                        [--rays N] [--rmax M] [--seed S] [--no-chosen] [--no-cpu-baseline]
        python bench.py --config surrogate [--train N] [--infer N] [--epochs E]
@@ -59,7 +62,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "PE grid-point updates/s (1 B200) plain vs chosen form at ≤0.1 dB TL RMS error"
 UNIT = "grid-point updates/s"
-B_ALG = {"plain": 72.0, "chosen": 52.0}  # algorithmic bytes per grid-point update
+B_ALG = {"plain": 72.0, "chosen": 52.0, "fast": 52.0}  # algorithmic bytes per grid-point update
 
 
 def parse():
@@ -68,7 +71,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--form", choices=["plain", "chosen"], default="plain")
+    ap.add_argument("--form", choices=["plain", "chosen", "fast"], default="plain")
     ap.add_argument("--config", choices=["munk", "pekeris", "wedge", "precision", "surrogate", "gemm", "peaks"],
                     default="munk")
     ap.add_argument("--train", type=int, default=200_000, help="surrogate: training marches")
@@ -247,9 +250,22 @@ def cpu_sample(batch, n_rays, seed, mode):
     pick = np.sort(rng.choice(batch.n_rays, size=n, replace=False))
     work = float(np.sum(batch.rays["nz"][pick].astype(np.float64) * batch.rays["nr"][pick]))
     t0 = time.perf_counter()
-    oracle.run(batch, mode, threads=min(cores, n), rays=pick)
+    ref = oracle.run(batch, mode, threads=min(cores, n), rays=pick)
     dt = time.perf_counter() - t0
-    return work / dt, dt, n, min(cores, n)
+    return work / dt, dt, n, min(cores, n), pick, ref
+
+
+def sample_parity(batch, pick, ref, tll):
+    """TL-line differences (dB) between a march's output `tll` and the oracle's
+    lines `ref` of the sampled rays `pick` (same ragged layout): max and RMS
+    over every output of those rays, plus the number of outputs compared."""
+    r = batch.rays[pick]
+    d = np.concatenate([np.abs(np.asarray(tll)[o:o + n] - ref["tll"][o:o + n])
+                        for o, n in zip(r["line_off"].tolist(), r["nvr"].tolist())])
+    if d.size == 0:
+        return {"rays": int(len(pick)), "outputs": 0, "max_db": None, "rms_db": None}
+    return {"rays": int(len(pick)), "outputs": int(d.size), "max_db": float(d.max()),
+            "rms_db": float(np.sqrt(np.mean(d * d)))}
 
 
 def tl_errors(tl_ref, tl):
@@ -259,11 +275,17 @@ def tl_errors(tl_ref, tl):
     return float(d.max()) if d.size else 0.0, float(np.sqrt(np.mean(d * d))) if d.size else 0.0
 
 
-def chosen_form(a, batch, out_plain, torch, world, pg, barrier, peak):
-    """Time the complex64 + FP32-sweep form on the same batch; TL errors against the plain run."""
+FORM_DESC = {"chosen": "complex64 factors and workspace, FP32 sweeps, FP64 term combination and field",
+             "fast": "complex64 factors and workspace, FP32 inner loop (sweeps, couplings, M u and term "
+                     "combination in FP32); FP64 factorisation and field"}
+
+
+def chosen_form(a, batch, out_plain, torch, world, pg, barrier, peak, form="chosen"):
+    """Time a reduced-precision form on the same batch; TL errors against the plain run.
+    Returns the bench record of the form and its TL line."""
     from cupyram_b200.engine import Engine
     refs = {k: out_plain[k].numpy().copy() for k in ("tll", "tlg") if k in out_plain}
-    eng = Engine(batch, precision="chosen")
+    eng = Engine(batch, precision=form)
     out = alloc_pinned(batch, torch)
     for _ in range(a.warmup):
         eng.run(out)
@@ -281,18 +303,19 @@ def chosen_form(a, batch, out_plain, torch, world, pg, barrier, peak):
         errs.update(tl_grid_err_max_db=gmax, tl_grid_err_rms_db=grms,
                     tl_grid_cells=int(np.sum(np.isfinite(refs["tlg"]) & (refs["tlg"] < 100.0))))
     eng.close()
+    tll_chosen = out["tll"].numpy().copy()
     pu = batch.point_updates
     value = whole_job_rate(sum_over_ranks(pg, pu), a.steps, t)
     per_launch_s = float(np.mean(ms)) * 1e-3
     achieved = pu * B_ALG["chosen"] / per_launch_s / 1e9
-    tpp = profiled_traffic("chosen") if a.config == "munk" else None
-    return {"form": "complex64 factors and workspace, FP32 sweeps, FP64 term combination and field",
+    tpp = profiled_traffic(form) if a.config == "munk" else None
+    return {"form": FORM_DESC[form], "precision": form,
             "value": value, "unit": UNIT, "ms_per_step": t / a.steps, **errs,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "bytes_per_point_update": B_ALG["chosen"],
                          "traffic": (tpp * pu) if tpp else None,
                          "traffic_gbs": (tpp * pu / per_launch_s / 1e9) if tpp else None,
-                         "traffic_frac": (tpp * pu / per_launch_s / 1e9 / peak) if tpp else None}}
+                         "traffic_frac": (tpp * pu / per_launch_s / 1e9 / peak) if tpp else None}}, tll_chosen
 
 
 def alloc_pinned(batch, torch):
@@ -312,7 +335,7 @@ def run_reference(a):
     batch, cfg = workload(a, 0)
     vals = []
     for k in range(a.warmup + a.steps):
-        v, dt, n, cores = cpu_sample(batch, a.cpu_rays, a.seed + k, "ref")
+        v, dt, n, cores, _, _ = cpu_sample(batch, a.cpu_rays, a.seed + k, "ref")
         if k >= a.warmup:
             vals.append((v, dt))
     value = float(np.mean([v for v, _ in vals]))
@@ -465,7 +488,6 @@ def main():
         pg = dist
     from cupyram_b200.engine import Engine
     batch, cfg = workload(a, rank)
-    eng = Engine(batch, precision=a.form)
     out = alloc_pinned(batch, torch)  # pinned host output buffers for the end-to-end path
 
     def barrier():
@@ -473,34 +495,48 @@ def main():
         if pg is not None:
             pg.barrier()
 
+    # Every step is the whole C-ABI call sequence a user makes for a batch:
+    # cr_create (validation, device Pade sets, tiling, device memory),
+    # cr_run (upload of the host batch, march, download of the TL / CP lines
+    # into pinned host buffers) and cr_destroy.  The march alone is timed on
+    # the device by CUDA events inside cr_march.
     for _ in range(a.warmup):
-        eng.run(out)
+        with Engine(batch, precision=a.form) as eng:
+            eng.run(out)
     barrier()
-    march_ms, e2e_ms, h2d_b, d2h_b, launches = [], [], 0, 0, 0
+    march_ms, e2e_ms, run_ms, create_ms, h2d_b, d2h_b, launches = [], [], [], [], 0, 0, 0
     with ClockSampler(local) as clk:
         for _ in range(a.steps):
             t0 = time.perf_counter()
+            eng = Engine(batch, precision=a.form)
+            t1 = time.perf_counter()
             eng.run(out)
-            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+            t2 = time.perf_counter()
             st = eng.stats()
+            eng.close()
+            e2e_ms.append((time.perf_counter() - t0) * 1e3)
+            run_ms.append((t2 - t1) * 1e3)
+            create_ms.append((t1 - t0) * 1e3)
             march_ms.append(st["march_ms"])
             h2d_b, d2h_b = st["h2d_bytes"], st["d2h_bytes"]
-            launches += st["kernel_launches"]
+            launches += st["kernel_launches"] + 1  # + the Pade launch of cr_create
     barrier()
-    t_march, t_e2e = max_over_ranks(pg, [float(np.sum(march_ms)), float(np.sum(e2e_ms))])
+    t_march, t_e2e, t_run = max_over_ranks(pg, [float(np.sum(march_ms)), float(np.sum(e2e_ms)),
+                                                float(np.sum(run_ms))])
     pu = batch.point_updates
     pu_all = sum_over_ranks(pg, pu)
     value = whole_job_rate(pu_all, a.steps, t_march)
     e2e = whole_job_rate(pu_all, a.steps, t_e2e)
+    e2e_resident = whole_job_rate(pu_all, a.steps, t_run)
     # sanity: every ray's line is finite
     tl = out["tll"].numpy()
     if not np.all(np.isfinite(tl)):
         raise RuntimeError("non-finite TL in the benchmark output")
-    eng.close()
     peak, peak_kind = measured_peak_hbm()
-    chosen = None
+    reduced = {}  # form -> (bench record, TL line)
     if a.form == "plain" and not a.no_chosen:  # every rank takes part (max-over-ranks timing)
-        chosen = chosen_form(a, batch, out, torch, world, pg, barrier, peak)
+        for form in ("chosen", "fast"):
+            reduced[form] = chosen_form(a, batch, out, torch, world, pg, barrier, peak, form)
     if rank != 0:
         if pg is not None:
             pg.destroy_process_group()
@@ -520,15 +556,25 @@ def main():
                          "traffic_gbs": (tpp * pu / per_launch_s / 1e9) if tpp else None,
                          "traffic_frac": (tpp * pu / per_launch_s / 1e9 / peak) if tpp else None},
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(h2d_b),
-                    "d2h_bytes_per_step": int(d2h_b)},
+                    "d2h_bytes_per_step": int(d2h_b),
+                    "calls": "cr_create + cr_run (upload, march, download to pinned host buffers) + cr_destroy",
+                    "create_ms_per_step": float(np.mean(create_ms))},
+            "e2e_resident": {"value": e2e_resident, "unit": UNIT,
+                             "calls": "cr_run on an engine already created (upload, march, download)"},
             "gpu_launches": int(launches), "clocks": clk.summary()}
-    if chosen is not None:
-        line["chosen"] = chosen
+    for form, (rec, _) in reduced.items():
+        line[form] = rec
     if world == 1 and not a.no_cpu_baseline:
-        v, dt, n, cores = cpu_sample(batch, a.cpu_rays, a.seed, "plain")
+        v, dt, n, cores, pick, ref = cpu_sample(batch, a.cpu_rays, a.seed, "plain")
         line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                                 "sample": f"{n} of the {batch.n_rays} rays, full march each, one ray "
                                           f"per core, {dt:.1f} s (C restatement in oracle/, FP64)"}
+        # the timed sample doubles as a parity check of this very batch: the
+        # march's TL lines of the sampled rays against the oracle's
+        line["parity"] = {"plain_vs_oracle": dict(sample_parity(batch, pick, ref, tl), bar_max_db=1e-3),
+                          "oracle": "plain complex128 C restatement, same rays, full range"}
+        for form, (_, tll_form) in reduced.items():
+            line["parity"][f"{form}_vs_oracle"] = dict(sample_parity(batch, pick, ref, tll_form), bar_rms_db=0.1)
     print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()

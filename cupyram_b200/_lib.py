@@ -19,7 +19,7 @@ MAX_NP = 10
 # status codes (enum cr_status)
 CR_OK, CR_EINVAL, CR_ECUDA, CR_EPADE, CR_ETIMEOUT, CR_ENAN, CR_ENOMEM, CR_ESTATE = range(8)
 # precision forms (enum cr_precision)
-CR_PLAIN_C128, CR_CHOSEN_C64R = 0, 1
+CR_PLAIN_C128, CR_CHOSEN_C64R, CR_CHOSEN_C64 = 0, 1, 2
 
 RAY_DTYPE = np.dtype(
     [("freq", "f8"), ("c0", "f8"), ("zs", "f8"), ("zr", "f8"), ("dz", "f8"), ("dr", "f8"),
@@ -61,6 +61,7 @@ _SIGS = {
     "cr_abi_version": (ctypes.c_int, []),
     "cr_pade": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
+    "cr_pade_batch": (ctypes.c_int, [ctypes.c_int] + [ctypes.c_void_p] * 10),
     "cr_create": (ctypes.c_int, [ctypes.POINTER(CrBatch), ctypes.POINTER(ctypes.c_void_p)]),
     "cr_upload": (ctypes.c_int, [ctypes.c_void_p]),
     "cr_march": (ctypes.c_int, [ctypes.c_void_p]),
@@ -75,6 +76,7 @@ _SIGS = {
     "cr_peak_fma": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                    ctypes.POINTER(ctypes.c_double)]),
     "cr_destroy": (None, [ctypes.c_void_p]),
+    "cr_release_cache": (ctypes.c_int, []),
     "cr_march_static": (ctypes.c_int, [ctypes.POINTER(CrBatch), ctypes.POINTER(CrOutputs), ctypes.c_void_p]),
     "cr_cell_tl": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_void_p]),

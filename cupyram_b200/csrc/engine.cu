@@ -650,11 +650,46 @@ struct cr_engine {
 
 namespace {
 
+// Device memory of the engines comes from one stream-ordered pool per device
+// that keeps freed memory for the next engine (release threshold: never), so
+// that building an engine for every batch - as CuPyRAM.run() does - costs no
+// fresh cudaMalloc / cudaFree after the first one.  cr_release_cache() hands
+// the pooled memory back to the device.
+constexpr int kPoolDevices = 64;
+cudaMemPool_t g_pools[kPoolDevices] = {};
+std::mutex g_pool_mu;
+
+cudaError_t engine_pool(int dev, cudaMemPool_t* out) {
+    if (dev < 0 || dev >= kPoolDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t pool = nullptr;
+        cudaError_t ce = cudaMemPoolCreate(&pool, &props);
+        if (ce != cudaSuccess) return ce;
+        unsigned long long keep = ~0ULL;
+        ce = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (ce != cudaSuccess) {
+            cudaMemPoolDestroy(pool);
+            return ce;
+        }
+        g_pools[dev] = pool;
+    }
+    *out = g_pools[dev];
+    return cudaSuccess;
+}
+
 template <typename T>
 cudaError_t dev_alloc(cr_engine* e, T** p, size_t count) {
     if (count == 0) count = 1;
     const size_t bytes = count * sizeof(T);
-    cudaError_t rc = cudaMalloc((void**)p, bytes);
+    cudaMemPool_t pool = nullptr;
+    cudaError_t rc = engine_pool(e->device, &pool);
+    if (rc == cudaSuccess) rc = cudaMallocFromPoolAsync((void**)p, bytes, pool, e->stream);
     if (rc == cudaSuccess) e->device_bytes += (long long)bytes;
     return rc;
 }
@@ -665,8 +700,13 @@ void free_all(cr_engine* e) {
                     e->d_tll,  e->d_cpl,  e->d_tlg,  e->d_cpg,      e->d_flags, e->d_S1, e->d_S2,
                     e->d_S3,   e->d_AL,   e->d_WF,   e->d_tile_G,  e->d_tile_off, e->d_tile_loff, e->d_pfc, e->d_pfcinf,
                     e->d_QD,   e->d_WD,   e->d_QU,   e->d_WU,      e->d_ED,  e->d_EU, e->d_col_ray};
-    for (void* p : ptrs)
-        if (p) cudaFree(p);
+    // stream-ordered frees on the engine's stream (every other stream of the
+    // engine joins it at the end of each march), back into the pool
+    if (e->stream) {
+        for (void* p : ptrs)
+            if (p) cudaFreeAsync(p, e->stream);
+        cudaStreamSynchronize(e->stream);
+    }
     for (auto& g : e->col_groups) {
         if (g.done) cudaEventDestroy(g.done);
         if (g.stream) cudaStreamDestroy(g.stream);
@@ -681,6 +721,64 @@ void free_all(cr_engine* e) {
     if (e->stream) cudaStreamDestroy(e->stream);
 }
 
+// Pinned staging of host-to-device copies.  A pageable cudaMemcpy is staged
+// by the driver through its own pinned buffers, one host copy at a time; here
+// each device has a ring of two pinned chunks, allocated once: while one
+// chunk's DMA runs, host threads fill the other, so the host copy and the
+// transfer overlap and the copy itself runs on several cores.
+constexpr size_t kStageChunk = 16u << 20;  // bytes per chunk
+constexpr size_t kStageMin = 4u << 20;     // smaller copies go direct
+constexpr int kStageThreads = 4;
+struct StageRing {
+    unsigned char* buf[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+};
+StageRing g_stage[kPoolDevices];
+std::mutex g_stage_mu[kPoolDevices];
+
+void copy_parallel(unsigned char* dst, const unsigned char* src, size_t n) {
+    if (n < (1u << 20)) {
+        memcpy(dst, src, n);
+        return;
+    }
+    std::thread th[kStageThreads - 1];
+    const size_t part = (n / kStageThreads + 63) & ~size_t(63);
+    for (int t = 1; t < kStageThreads; ++t) {
+        const size_t lo = std::min(n, part * t), hi = std::min(n, part * (t + 1));
+        th[t - 1] = std::thread([=] { memcpy(dst + lo, src + lo, hi - lo); });
+    }
+    memcpy(dst, src, std::min(n, part));
+    for (auto& x : th) x.join();
+}
+
+// Host-to-device copy of `bytes` through the device's pinned ring, ordered on
+// `st`.  Returns when the last chunk's copy has been queued (the caller
+// synchronises the stream); the ring is held until then.
+cudaError_t staged_h2d(int dev, void* dst, const void* src, size_t bytes, cudaStream_t st) {
+    if (dev < 0 || dev >= kPoolDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_stage_mu[dev]);
+    StageRing& R = g_stage[dev];
+    cudaError_t ce = cudaSuccess;
+    for (int k = 0; k < 2 && ce == cudaSuccess; ++k) {
+        if (!R.buf[k]) ce = cudaHostAlloc((void**)&R.buf[k], kStageChunk, cudaHostAllocPortable);
+        if (ce == cudaSuccess && !R.done[k]) ce = cudaEventCreateWithFlags(&R.done[k], cudaEventDisableTiming);
+    }
+    const unsigned char* s = (const unsigned char*)src;
+    unsigned char* d = (unsigned char*)dst;
+    int k = 0;
+    for (size_t off = 0; off < bytes && ce == cudaSuccess; off += kStageChunk, k ^= 1) {
+        const size_t n = std::min(kStageChunk, bytes - off);
+        ce = cudaEventSynchronize(R.done[k]);  // the chunk's previous DMA has finished
+        if (ce != cudaSuccess) break;
+        copy_parallel(R.buf[k], s + off, n);
+        ce = cudaMemcpyAsync(d + off, R.buf[k], n, cudaMemcpyHostToDevice, st);
+        if (ce == cudaSuccess) ce = cudaEventRecord(R.done[k], st);
+    }
+    // the ring is reused by the next call only after these copies: wait for them
+    for (int j = 0; j < 2 && ce == cudaSuccess; ++j) ce = cudaEventSynchronize(R.done[j]);
+    return ce;
+}
+
 // Validate the batch; returns an error message or empty string.
 std::string validate(const cr_batch* b) {
     char buf[256];
@@ -688,7 +786,8 @@ std::string validate(const cr_batch* b) {
     if (b->n_rays < 1) return "n_rays must be >= 1";
     if (b->n_envs < 1) return "n_envs must be >= 1";
     if (!b->rays || !b->envs || !b->pool) return "rays, envs and pool must be non-NULL";
-    if (b->precision != CR_PLAIN_C128 && b->precision != CR_CHOSEN_C64R) return "unknown precision form";
+    if (b->precision != CR_PLAIN_C128 && b->precision != CR_CHOSEN_C64R && b->precision != CR_CHOSEN_C64)
+        return "unknown precision form";
     for (int k = 0; k < b->n_envs; ++k) {
         const cr_env& v = b->envs[k];
         if (v.n_zss < 1 || v.n_rss < 1 || v.n_zsb < 1 || v.n_rsb < 1 || v.n_bt < 1) {
@@ -727,7 +826,71 @@ std::string validate(const cr_batch* b) {
     return std::string();
 }
 
-// Pade sets for every ray; identical (freq, c0, np, ns, dr) share one solve.
+// One Pade solve of a batch: (freq, c0, dr, np, ns, ip).
+struct PadeJob {
+    double freq, c0, dr;
+    int np, ns, ip, pad_;
+};
+
+// One thread per job: the FP64 Pade construction of pade.h on the device.
+// pd1 / pd2 get CR_MAX_NP coefficients per job (zeros past np); status gets
+// CR_OK, CR_EPADE (Laguerre did not converge) or CR_EINVAL.
+__global__ void pade_batch_kernel(const PadeJob* __restrict__ jobs, int n, double2* __restrict__ pd1,
+                                  double2* __restrict__ pd2, int* __restrict__ status) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const PadeJob j = jobs[i];
+    cr::cd a[CR_MAX_NP], c[CR_MAX_NP];
+    const int rc = cr::pade_coefficients(j.freq, j.c0, j.np, j.ns, j.dr, j.ip, a, c);
+    status[i] = rc == cr::kPadeOk ? CR_OK : (rc == cr::kPadeNoConverge ? CR_EPADE : CR_EINVAL);
+    for (int k = 0; k < CR_MAX_NP; ++k) {
+        const bool on = rc == cr::kPadeOk && k < j.np;
+        pd1[(size_t)i * CR_MAX_NP + k] = on ? make_double2(a[k].re, a[k].im) : make_double2(0.0, 0.0);
+        pd2[(size_t)i * CR_MAX_NP + k] = on ? make_double2(c[k].re, c[k].im) : make_double2(0.0, 0.0);
+    }
+}
+
+// Solve a batch of Pade jobs on the current device (temporary device memory
+// on a private stream; synchronous).  pd1 / pd2: [n][CR_MAX_NP], status: [n].
+cudaError_t device_pade(const std::vector<PadeJob>& jobs, std::vector<double2>& pd1, std::vector<double2>& pd2,
+                        std::vector<int>& status) {
+    const int n = (int)jobs.size();
+    pd1.assign((size_t)n * CR_MAX_NP, make_double2(0.0, 0.0));
+    pd2.assign((size_t)n * CR_MAX_NP, make_double2(0.0, 0.0));
+    status.assign((size_t)n, CR_OK);
+    if (n == 0) return cudaSuccess;
+    cudaStream_t st = nullptr;
+    cudaError_t ce = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    if (ce != cudaSuccess) return ce;
+    const size_t bj = jobs.size() * sizeof(PadeJob), bp = pd1.size() * sizeof(double2), bs = (size_t)n * sizeof(int);
+    unsigned char* d = nullptr;
+    ce = cudaMallocAsync((void**)&d, bj + 2 * bp + bs, st);
+    if (ce == cudaSuccess) {
+        PadeJob* dj = (PadeJob*)d;
+        double2* d1 = (double2*)(d + bj);
+        double2* d2 = (double2*)(d + bj + bp);
+        int* ds = (int*)(d + bj + 2 * bp);
+        ce = cudaMemcpyAsync(dj, jobs.data(), bj, cudaMemcpyHostToDevice, st);
+        if (ce == cudaSuccess) {
+            // 32 threads a block: the solves are long serial chains, so the
+            // jobs are spread over as many SMs as possible
+            pade_batch_kernel<<<(n + 31) / 32, 32, 0, st>>>(dj, n, d1, d2, ds);
+            ce = cudaGetLastError();
+        }
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(pd1.data(), d1, bp, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(pd2.data(), d2, bp, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(status.data(), ds, bs, cudaMemcpyDeviceToHost, st);
+        const cudaError_t cf = cudaFreeAsync(d, st);
+        if (ce == cudaSuccess) ce = cf;
+    }
+    const cudaError_t cs = cudaStreamSynchronize(st);
+    if (ce == cudaSuccess) ce = cs;
+    cudaStreamDestroy(st);
+    return ce;
+}
+
+// Pade sets for every ray, solved on the device; identical (freq, c0, np,
+// ns, dr) share one solve.
 int compute_pade_sets(cr_engine* e, const cr_batch* b) {
     using Key = std::tuple<double, double, int, int, double>;
     std::map<Key, int> uniq;
@@ -744,50 +907,44 @@ int compute_pade_sets(cr_engine* e, const cr_batch* b) {
         ray_key[i] = it->second;
     }
     const int nk = (int)keys.size();
-    // per key: set1 (ip=2), set2 (ip=1, ns), set3 (ip=1, ns=0)
-    std::vector<cr::cd> res((size_t)nk * 3 * 2 * CR_MAX_NP);
-    std::vector<int> status(nk, 0);
-    std::atomic<int> next{0};
-    auto work = [&]() {
-        for (;;) {
-            const int k = next.fetch_add(1);
-            if (k >= nk) return;
-            const auto& [freq, c0, np, ns, dr] = keys[k];
-            cr::cd* base = res.data() + (size_t)k * 3 * 2 * CR_MAX_NP;
-            int rc = cr::pade_coefficients(freq, c0, np, ns, dr, 2, base, base + CR_MAX_NP);
-            if (!rc) rc = cr::pade_coefficients(freq, c0, np, ns, dr, 1, base + 2 * CR_MAX_NP, base + 3 * CR_MAX_NP);
-            if (!rc) rc = cr::pade_coefficients(freq, c0, np, 0, dr, 1, base + 4 * CR_MAX_NP, base + 5 * CR_MAX_NP);
-            status[k] = rc;
-        }
-    };
-    const int nthr = std::max(1, std::min<int>(nk / 16, (int)std::thread::hardware_concurrency()));
-    std::vector<std::thread> th;
-    for (int t = 1; t < nthr; ++t) th.emplace_back(work);
-    work();
-    for (auto& t : th) t.join();
+    // per key: set1 (ip=2, ns), set2 (ip=1, ns), set3 (ip=1, ns=0)
+    std::vector<PadeJob> jobs((size_t)nk * 3);
+    for (int k = 0; k < nk; ++k) {
+        const auto& [freq, c0, np, ns, dr] = keys[k];
+        jobs[(size_t)k * 3 + 0] = PadeJob{freq, c0, dr, np, ns, 2, 0};
+        jobs[(size_t)k * 3 + 1] = PadeJob{freq, c0, dr, np, ns, 1, 0};
+        jobs[(size_t)k * 3 + 2] = PadeJob{freq, c0, dr, np, 0, 1, 0};
+    }
+    std::vector<double2> r1, r2;
+    std::vector<int> status;
+    const cudaError_t ce = device_pade(jobs, r1, r2, status);
+    if (ce != cudaSuccess)
+        return e->fail(ce == cudaErrorMemoryAllocation ? CR_ENOMEM : CR_ECUDA, "cr_create: Pade on the device: %s",
+                       cudaGetErrorString(ce));
     for (int k = 0; k < nk; ++k)
-        if (status[k]) {
-            const auto& [freq, c0, np, ns, dr] = keys[k];
-            return e->fail(CR_EPADE, "Pade coefficients failed (freq=%g c0=%g np=%d ns=%d dr=%g): %s", freq,
-                           c0, np, ns, dr, status[k] == cr::kPadeNoConverge ? "Laguerre method not converging" : "bad arguments");
-        }
+        for (int s = 0; s < 3; ++s)
+            if (status[(size_t)k * 3 + s] != CR_OK) {
+                const auto& [freq, c0, np, ns, dr] = keys[k];
+                return e->fail(status[(size_t)k * 3 + s] == CR_EPADE ? CR_EPADE : CR_EINVAL,
+                               "Pade coefficients failed (freq=%g c0=%g np=%d ns=%d dr=%g): %s", freq, c0, np, ns,
+                               dr, status[(size_t)k * 3 + s] == CR_EPADE ? "Laguerre method not converging"
+                                                                          : "bad arguments");
+            }
     e->pd1.assign((size_t)b->n_rays * kSets * CR_MAX_NP, make_double2(0.0, 0.0));
     e->pd2.assign((size_t)b->n_rays * kSets * CR_MAX_NP, make_double2(0.0, 0.0));
     e->pd_n.assign((size_t)b->n_rays * kSets, 0);
     for (int i = 0; i < b->n_rays; ++i) {
         const int np = b->rays[i].np;
-        const cr::cd* base = res.data() + (size_t)ray_key[i] * 3 * 2 * CR_MAX_NP;
         double2* p1 = e->pd1.data() + (size_t)i * kSets * CR_MAX_NP;
         double2* p2 = e->pd2.data() + (size_t)i * kSets * CR_MAX_NP;
         p1[0] = make_double2(0.0, 0.0);
         p2[0] = make_double2(-1.0, 0.0);
         e->pd_n[i * kSets + 0] = 1;
         for (int s = 1; s < kSets; ++s) {
-            const cr::cd* a1 = base + (size_t)(s - 1) * 2 * CR_MAX_NP;
-            const cr::cd* a2 = a1 + CR_MAX_NP;
+            const size_t jb = ((size_t)ray_key[i] * 3 + (s - 1)) * CR_MAX_NP;
             for (int j = 0; j < np; ++j) {
-                p1[s * CR_MAX_NP + j] = make_double2(a1[j].re, a1[j].im);
-                p2[s * CR_MAX_NP + j] = make_double2(a2[j].re, a2[j].im);
+                p1[s * CR_MAX_NP + j] = r1[jb + j];
+                p2[s * CR_MAX_NP + j] = r2[jb + j];
             }
             e->pd_n[i * kSets + s] = np;
         }
@@ -840,6 +997,46 @@ int cr_pade(double freq, double c0, int np, int ns, double dr, int ip, double* p
         pd2[2 * j + 1] = b[j].im;
     }
     return CR_OK;
+}
+
+int cr_pade_batch(int n, const double* freq, const double* c0, const int32_t* np, const int32_t* ns,
+                  const double* dr, const int32_t* ip, double* pd1, double* pd2, int32_t* status) {
+    NvtxRange nv("cr_pade_batch");
+    if (n < 0 || (n > 0 && (!freq || !c0 || !np || !ns || !dr || !ip || !pd1 || !pd2 || !status))) {
+        set_global_error("cr_pade_batch: invalid arguments");
+        return CR_EINVAL;
+    }
+    std::vector<PadeJob> jobs((size_t)n);
+    for (int i = 0; i < n; ++i) {
+        if (np[i] < 1 || np[i] > CR_MAX_NP || ns[i] < 0 || ns[i] > 2 || (ip[i] != 1 && ip[i] != 2)) {
+            set_global_error("cr_pade_batch: job %d: invalid arguments (np=%d ns=%d ip=%d)", i, np[i], ns[i], ip[i]);
+            return CR_EINVAL;
+        }
+        jobs[(size_t)i] = PadeJob{freq[i], c0[i], dr[i], np[i], ns[i], ip[i], 0};
+    }
+    std::vector<double2> r1, r2;
+    std::vector<int> st;
+    const cudaError_t ce = device_pade(jobs, r1, r2, st);
+    if (ce != cudaSuccess) {
+        set_global_error("cr_pade_batch: %s", cudaGetErrorString(ce));
+        return ce == cudaErrorMemoryAllocation ? CR_ENOMEM : CR_ECUDA;
+    }
+    int worst = CR_OK;
+    for (int i = 0; i < n; ++i) {
+        status[i] = st[(size_t)i];
+        if (st[(size_t)i] != CR_OK && worst == CR_OK) {
+            worst = st[(size_t)i];
+            set_global_error("cr_pade_batch: job %d: %s", i,
+                             worst == CR_EPADE ? "Laguerre method not converging" : "invalid arguments");
+        }
+        for (int j = 0; j < CR_MAX_NP; ++j) {  // zeros past np[i]
+            pd1[2 * ((size_t)i * CR_MAX_NP + j)] = r1[(size_t)i * CR_MAX_NP + j].x;
+            pd1[2 * ((size_t)i * CR_MAX_NP + j) + 1] = r1[(size_t)i * CR_MAX_NP + j].y;
+            pd2[2 * ((size_t)i * CR_MAX_NP + j)] = r2[(size_t)i * CR_MAX_NP + j].x;
+            pd2[2 * ((size_t)i * CR_MAX_NP + j) + 1] = r2[(size_t)i * CR_MAX_NP + j].y;
+        }
+    }
+    return worst;
 }
 
 namespace {
@@ -1056,7 +1253,7 @@ int cr_create(const cr_batch* b, cr_engine** out) {
             if ((int)std::floor(b->rays[i].zs / b->rays[i].dz) < 1) ok = false;
         e->sum_mode = ok;
     }
-    if (b->precision == CR_CHOSEN_C64R && !e->sum_mode) {
+    if (b->precision != CR_PLAIN_C128 && !e->sum_mode) {
         set_global_error("cr_create: the chosen complex64 form needs every source below the first depth cell "
                          "(zs >= dz) and the partial-fraction march (CUPYRAM_B200_SUM != 0)");
         delete e;
@@ -1078,7 +1275,7 @@ int cr_create(const cr_batch* b, cr_engine** out) {
         return wx > wy;
     });
     if (e->sum_mode) {
-        const std::vector<char> is_col = pick_column_rays(b, e->pd_n, b->precision == CR_CHOSEN_C64R);
+        const std::vector<char> is_col = pick_column_rays(b, e->pd_n, b->precision != CR_PLAIN_C128);
         // batched rays grouped by Pade order, then work; a tile holds
         // floor(32/G) rays of G lanes each, G = the largest np in the tile
         std::vector<int> bord;
@@ -1146,7 +1343,7 @@ int cr_create(const cr_batch* b, cr_engine** out) {
         for (int rid : order)
             if (is_col[(size_t)rid]) cord.push_back(rid);
         auto terms_of = [&](int rid) { return col_terms(e->pd_n, rid); };
-        const bool chosen = b->precision == CR_CHOSEN_C64R;
+        const bool chosen = b->precision != CR_PLAIN_C128;
         const std::vector<int> csize = column_clusters(b, e->pd_n, is_col, chosen);
         std::stable_sort(cord.begin(), cord.end(), [&](int x, int y) {
             const int tx = terms_of(x), ty = terms_of(y);
@@ -1353,7 +1550,11 @@ int cr_upload(cr_engine* e) {
     float ms = 0.f;
     if (ce == cudaSuccess) ce = cudaEventRecord(e->ev[0], e->stream);
     auto cp = [&](void* dst, const void* src, size_t bytes) {
-        if (ce == cudaSuccess && bytes) ce = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, e->stream);
+        if (ce != cudaSuccess || !bytes) return;
+        // large arrays (the environment pool) go through the pinned staging
+        // ring; small tables are copied directly
+        ce = bytes >= kStageMin ? staged_h2d(e->device, dst, src, bytes, e->stream)
+                                : cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, e->stream);
     };
     cp(e->d_rays, e->rays.data(), e->rays.size() * sizeof(RayDev));
     cp(e->d_envs, e->envs.data(), e->envs.size() * sizeof(EnvDev));
@@ -1465,7 +1666,7 @@ int cr_march(cr_engine* e) {
         ca.cpg = e->d_cpg;
         ca.flags = e->d_flags;
         ca.compute_grids = e->compute_grids;
-        const int chosen = e->precision == CR_CHOSEN_C64R;
+        const int chosen = e->precision != CR_PLAIN_C128;
         ce = cudaEventRecord(e->ev[0], e->stream);
         int nl = 0;
         // column groups first, each on its own stream (they hold the longest
@@ -1484,7 +1685,7 @@ int cr_march(cr_engine* e) {
         sa.tile_begin = 0;
         int nb = 0;
         if (ce == cudaSuccess)
-            ce = crk::launch_march_sum(sa, e->tile_G.data(), e->n_tiles, chosen, e->sum_streams.data(),
+            ce = crk::launch_march_sum(sa, e->tile_G.data(), e->n_tiles, e->precision, e->sum_streams.data(),
                                        (int)e->sum_streams.size(), &nb);
         for (size_t i = 1; i < e->sum_streams.size(); ++i) {
             if (ce == cudaSuccess) ce = cudaEventRecord(e->sum_done[i], e->sum_streams[i]);
@@ -1639,6 +1840,19 @@ void cr_destroy(cr_engine* e) {
     delete e;
 }
 
+int cr_release_cache(void) {
+    std::lock_guard<std::mutex> lock(g_pool_mu);
+    for (int d = 0; d < kPoolDevices; ++d) {
+        if (!g_pools[d]) continue;
+        const cudaError_t ce = cudaMemPoolTrimTo(g_pools[d], 0);
+        if (ce != cudaSuccess) {
+            set_global_error("cr_release_cache: %s", cudaGetErrorString(ce));
+            return CR_ECUDA;
+        }
+    }
+    return CR_OK;
+}
+
 }  // extern "C"
 
 // ===========================================================================
@@ -1660,24 +1874,53 @@ static_assert(sizeof(cr_env) == sizeof(EnvDev), "cr_env and EnvDev must share a 
 static_assert(sizeof(cr_ray) == 136, "cr_ray layout changed");
 
 // Device address of g_static_scratch per device, looked up on the first call
-// on that device (host code cannot use the symbol's name as an address).
+// on that device (host code cannot use the symbol's name as an address).  The
+// address belongs to the device's current context: it is stored with that
+// context's handle and looked up again when the context changes (after a
+// cudaDeviceReset, for example), so a stale address is never used.
 constexpr int kMaxDevices = 64;
-void* g_static_ptr[kMaxDevices] = {};
+struct StaticPtr {
+    void* ctx = nullptr;
+    void* ptr = nullptr;
+};
+StaticPtr g_static_ptr[kMaxDevices];
 std::mutex g_static_mu;
+
+// Handle of the calling thread's current CUDA context, through the driver
+// entry point the runtime exposes (nullptr when it is unavailable; the
+// address is then looked up on every call).
+void* current_context() {
+    using Fn = int (*)(void**);  // CUresult cuCtxGetCurrent(CUcontext*)
+    static Fn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (Fn)p;
+    });
+    void* ctx = nullptr;
+    if (!fn || fn(&ctx) != 0) return nullptr;
+    return ctx;
+}
 
 int static_scratch_ptr(int dev, void** out) {
     if (dev < 0 || dev >= kMaxDevices) return CR_EINVAL;
     std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_ptr[dev]) {
+    void* ctx = current_context();
+    StaticPtr& c = g_static_ptr[dev];
+    if (!c.ptr || !ctx || c.ctx != ctx) {
         void* p = nullptr;
         const cudaError_t ce = cudaGetSymbolAddress(&p, g_static_scratch);
         if (ce != cudaSuccess || !p) {
             set_global_error("cr_march_static: cudaGetSymbolAddress failed: %s", cudaGetErrorString(ce));
             return CR_ECUDA;
         }
-        g_static_ptr[dev] = p;
+        c.ptr = p;
+        c.ctx = ctx;
     }
-    *out = g_static_ptr[dev];
+    *out = c.ptr;
     return CR_OK;
 }
 
@@ -1731,7 +1974,6 @@ __global__ void static_setup_kernel(const cr_ray* raw, int n_rays, int compute_g
                                     int* tile_ray, double2* pd1, double2* pd2, int* pd_n, int* flags, int* status,
                                     int n_slots) {
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b == 0) *status = 0;
     if (b >= n_slots) return;
     if (b >= n_rays) {
         tile_ray[b] = -1;
@@ -1849,6 +2091,9 @@ extern "C" int cr_march_static(const cr_batch* b, const cr_outputs* out, void* s
     h2d(L.envs, b->envs, (size_t)b->n_envs * sizeof(cr_env));
     h2d(L.pool, b->pool, (size_t)b->pool_len * sizeof(double));
     const int n_slots = L.n_tiles * kTile;
+    // The status word is cleared on the stream before any thread of the set-up
+    // kernel can set a bit in it (no in-kernel clear: blocks run in no fixed order).
+    if (ce == cudaSuccess) ce = cudaMemsetAsync(base + L.status, 0, sizeof(int), st);
     if (ce == cudaSuccess) {
         static_setup_kernel<<<(n_slots + 127) / 128, 128, 0, st>>>(
             (const cr_ray*)(base + L.rays_raw), b->n_rays, b->compute_grids, L.rows, (RayDev*)(base + L.rays),

@@ -59,10 +59,51 @@ struct SumSmem {
 
 enum SumPass { kElimOnly = 0, kFusedP = 1, kBackOnly = 2, kFactor = 3 };
 
-// Sweep precision: plain = complex128 factors / workspace and FP64
-// recurrences; chosen = complex64 factors / workspace and FP32 recurrences.
-// The factorisation itself, the combination of the terms and the stored
-// field stay FP64 / complex128 in both forms.
+// Arithmetic forms of the march (template parameter F):
+//   kPlain  (0): complex128 factors / workspace, FP64 recurrences;
+//   kChosen (1): complex64 factors / workspace, FP32 recurrences, the terms
+//                combined in FP64 and the history of the field in FP64;
+//   kFast   (2): complex64 factors / workspace and an FP32 inner loop: the
+//                elimination's coupling, M u, the term combination and the
+//                exchange of the ray's shares all in FP32, the couplings
+//                stored as complex64.
+// The factorisation itself and the stored field stay FP64 / complex128 in
+// every form.
+constexpr int kPlain = 0, kChosen = 1, kFast = 2;
+template <int F>
+struct Form;
+template <>
+struct Form<kPlain> {
+    using R = double;
+    using V = double2;  // factors / workspace / recurrences
+    using H = double2;  // field history and term combination
+    using E = double2;  // stored Galerkin coupling
+};
+template <>
+struct Form<kChosen> {
+    using R = float;
+    using V = float2;
+    using H = double2;
+    using E = double2;
+};
+template <>
+struct Form<kFast> {
+    using R = float;
+    using V = float2;
+    using H = float2;
+    using E = float2;
+};
+
+__device__ __forceinline__ double2 up2(double2 v) { return v; }
+__device__ __forceinline__ double2 up2(float2 v) { return make_double2((double)v.x, (double)v.y); }
+template <typename T>
+__device__ __forceinline__ T dn2(double2 v);
+template <>
+__device__ __forceinline__ double2 dn2<double2>(double2 v) { return v; }
+template <>
+__device__ __forceinline__ float2 dn2<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+
+// Prec<R>: the stored precision of the factors / workspace.
 template <typename R>
 struct Prec;
 template <>
@@ -77,17 +118,6 @@ struct Prec<float> {
     __device__ static __forceinline__ V mk(double2 v) { return make_float2((float)v.x, (float)v.y); }
     __device__ static __forceinline__ double2 up(V v) { return make_double2((double)v.x, (double)v.y); }
 };
-
-template <typename R>
-__device__ __forceinline__ void cpv(void* dst, const void* src) {
-    if (sizeof(R) == 8) cp16(dst, src);
-    else cp8(dst, src);
-}
-template <typename R>
-__device__ __forceinline__ void cpvz(void* dst, const void* src, bool on) {
-    if (sizeof(R) == 8) cp16z(dst, src, on);
-    else cp8z(dst, src, on);
-}
 
 struct Lane {
     int lane, k, gbase, P;  // k: lane index within the ray's P lanes
@@ -107,6 +137,9 @@ struct Ops {
     double2 pole[kT];  // pd2 of this lane's terms in the active set
     double2 ck[kT];    // partial-fraction residues (0 for slots without a term)
     double2 cinf;      // c_inf of the ray for the active set
+    // FP32 copies for the fast form's inner loop
+    float a1f, a2f;
+    float2 polef[kT], ckf[kT], cinff;
 };
 
 template <typename R>
@@ -129,7 +162,7 @@ __device__ __forceinline__ int row_of(const Lane& L, int k) {
 
 // Copies for stream row r of a factor pass (one commit group, empty outside
 // the lane's rows).
-template <typename R, int PASS, bool DOWN>
+template <bool DOWN>
 __device__ __forceinline__ void sum_issue(const SumArgs& a, const Lane& L, SumSmem& S, int slot, int r, int nz) {
     if (r >= 0 && r <= nz + 1) {
         const long long ro = L.rcol + (long long)r * kTile;
@@ -143,21 +176,24 @@ __device__ __forceinline__ void sum_issue(const SumArgs& a, const Lane& L, SumSm
 }
 
 // Column pointers of one solve pass (element 0 of the lane's columns).
-template <typename R>
+template <int F>
 struct PassPtrs {
-    using V = typename Prec<R>::V;
+    using V = typename Form<F>::V;
+    using E = typename Form<F>::E;
     double2* u;        // field (ray column)
-    const double2* e;  // Galerkin coupling of this pass's elimination (ray column)
+    const E* e;        // Galerkin coupling of this pass's elimination (ray column)
     const V* w[kT];    // w of the solves being back-substituted (eliminated the other way)
     V* g[kT];          // workspace: read by the back-substitution, rewritten by the elimination
     const V* q[kT];    // 1/den of this pass's elimination
 };
 
-template <typename R, bool DOWN>
-__device__ __forceinline__ PassPtrs<R> pass_ptrs(const SumArgs& a, const Lane& L) {
-    PassPtrs<R> p;
+template <int F, bool DOWN>
+__device__ __forceinline__ PassPtrs<F> pass_ptrs(const SumArgs& a, const Lane& L) {
+    using R = typename Form<F>::R;
+    using E = typename Form<F>::E;
+    PassPtrs<F> p;
     p.u = a.u + L.rcol;
-    p.e = (DOWN ? a.ED : a.EU) + L.rcol;
+    p.e = reinterpret_cast<const E*>(DOWN ? a.ED : a.EU) + L.rcol;
 #pragma unroll
     for (int t = 0; t < kT; ++t) {
         const long long lo = L.lcol + t * L.lstride;
@@ -168,14 +204,27 @@ __device__ __forceinline__ PassPtrs<R> pass_ptrs(const SumArgs& a, const Lane& L
     return p;
 }
 
+template <typename T>
+__device__ __forceinline__ void cpt(void* dst, const void* src) {
+    if (sizeof(T) == 16) cp16(dst, src);
+    else cp8(dst, src);
+}
+template <typename T>
+__device__ __forceinline__ void cptz(void* dst, const void* src, bool on) {
+    if (sizeof(T) == 16) cp16z(dst, src, on);
+    else cp8z(dst, src, on);
+}
+
 // Copies for stream row r of a solve pass (one commit group).  The
 // elimination works two rows behind the stream (row m = r -/+ 2).  CHECK:
 // rows outside the lane's column are copied with zero source size (no
 // global read; the slot is zero-filled).  Without CHECK every row involved
 // is an interior row of every ray of the warp.
-template <typename R, int PASS, bool DOWN, bool CHECK>
-__device__ __forceinline__ void solve_issue(const PassPtrs<R>& p, const Lane& L, SumSmem& S, int slot, int r,
+template <int F, int PASS, bool DOWN, bool CHECK>
+__device__ __forceinline__ void solve_issue(const PassPtrs<F>& p, const Lane& L, SumSmem& S, int slot, int r,
                                             int nz) {
+    using V = typename Form<F>::V;
+    using E = typename Form<F>::E;
     const bool on = CHECK ? ((r >= 0) & (r <= nz + 1)) : true;
     const int ro = (CHECK ? (on ? r : 0) : r) * kTile;
     const bool uon = PASS == kElimOnly ? on : (on & (L.k == 0));
@@ -185,42 +234,46 @@ __device__ __forceinline__ void solve_issue(const PassPtrs<R>& p, const Lane& L,
     const bool mon = CHECK ? (on & (m >= 1) & (m <= nz)) : true;
     const int mo = (CHECK ? (mon ? m : 0) : m) * kTile;
     if (PASS != kBackOnly) {
-        if (CHECK) cp16z(&S.q[slot][1][L.lane], p.e + mo, mon);
-        else cp16(&S.q[slot][1][L.lane], p.e + mo);
+        if (CHECK) cptz<E>(&S.q[slot][1][L.lane], p.e + mo, mon);
+        else cpt<E>(&S.q[slot][1][L.lane], p.e + mo);
     }
 #pragma unroll
     for (int t = 0; t < kT; ++t) {
         if (PASS != kElimOnly) {
             if (CHECK) {
-                cpvz<R>(&S.q[slot][2 + 3 * t][L.lane], p.w[t] + ro, on);
-                cpvz<R>(&S.q[slot][3 + 3 * t][L.lane], p.g[t] + ro, on);
+                cptz<V>(&S.q[slot][2 + 3 * t][L.lane], p.w[t] + ro, on);
+                cptz<V>(&S.q[slot][3 + 3 * t][L.lane], p.g[t] + ro, on);
             } else {
-                cpv<R>(&S.q[slot][2 + 3 * t][L.lane], p.w[t] + ro);
-                cpv<R>(&S.q[slot][3 + 3 * t][L.lane], p.g[t] + ro);
+                cpt<V>(&S.q[slot][2 + 3 * t][L.lane], p.w[t] + ro);
+                cpt<V>(&S.q[slot][3 + 3 * t][L.lane], p.g[t] + ro);
             }
         }
         if (PASS != kBackOnly) {
-            if (CHECK) cpvz<R>(&S.q[slot][4 + 3 * t][L.lane], p.q[t] + mo, mon);
-            else cpv<R>(&S.q[slot][4 + 3 * t][L.lane], p.q[t] + mo);
+            if (CHECK) cptz<V>(&S.q[slot][4 + 3 * t][L.lane], p.q[t] + mo, mon);
+            else cpt<V>(&S.q[slot][4 + 3 * t][L.lane], p.q[t] + mo);
         }
     }
     cp_commit();
 }
 
 // Thomas factorisation of (M + pole_t D) for this lane's terms, one direction.
-template <typename R, bool DOWN>
+// The arithmetic is FP64 in every form; 1/den and w are stored in the sweep
+// precision, the row's Galerkin coupling in the form's coupling precision.
+template <int F, bool DOWN>
 __device__ void sum_factor(const SumArgs& a, const Lane& L, SumSmem& S, const Ops& o) {
+    using R = typename Form<F>::R;
+    using E = typename Form<F>::E;
     using P = Prec<R>;
     const int nz = o.nz;
     __threadfence_block();
 #pragma unroll 1
-    for (int k = 0; k < kSR; ++k) sum_issue<R, kFactor, DOWN>(a, L, S, k, row_of<DOWN>(L, k), nz);
+    for (int k = 0; k < kSR; ++k) sum_issue<DOWN>(a, L, S, k, row_of<DOWN>(L, k), nz);
     EnvRow em{}, ec{}, ep{};
     double2 wp[kT];
 #pragma unroll
     for (int t = 0; t < kT; ++t) wp[t] = c2(0.0, 0.0);
     typename P::V* Q = facw<R>(DOWN ? a.QD : a.QU);
-    double2* E = DOWN ? a.ED : a.EU;
+    E* Ecol = reinterpret_cast<E*>(DOWN ? a.ED : a.EU);
     typename P::V* W = facw<R>(DOWN ? a.WD : a.WU);
     int seen = 0;  // rows of this lane already streamed
 #pragma unroll 1
@@ -236,7 +289,7 @@ __device__ void sum_factor(const SumArgs& a, const Lane& L, SumSmem& S, const Op
             er.f3 = f[2];
             er.k = *sks(S, slot, L.lane);
         }
-        sum_issue<R, kFactor, DOWN>(a, L, S, slot, row_of<DOWN>(L, k + kSR), nz);
+        sum_issue<DOWN>(a, L, S, slot, row_of<DOWN>(L, k + kSR), nz);
         if (r < 0 || r > nz + 1) continue;
         if (DOWN) {
             em = ec;
@@ -251,7 +304,7 @@ __device__ void sum_factor(const SumArgs& a, const Lane& L, SumSmem& S, const Op
         const int m = DOWN ? r - 1 : r + 1;
         if (m < 1 || m > nz) continue;
         const Drow d = galerkin3(em, ec, ep, o.cfact);
-        if (L.k == 0) E[L.rcol + (long long)m * kTile] = DOWN ? d.d1 : d.d3;
+        if (L.k == 0) Ecol[L.rcol + (long long)m * kTile] = dn2<E>(DOWN ? d.d1 : d.d3);
 #pragma unroll
         for (int t = 0; t < kT; ++t) {
             const double2 r1 = caxpd(o.a1, o.pole[t], d.d1), r2 = caxpd(o.a2, o.pole[t], d.d2),
@@ -270,40 +323,61 @@ __device__ void sum_factor(const SumArgs& a, const Lane& L, SumSmem& S, const Op
 // g_m = q (M u)_m + al g_{m-/+1} for every term slot of the lane, with the
 // coupling factor al = -(a1 + pole e) q rebuilt from the stored 1/den q and
 // the row's Galerkin coupling e (the factorisation's own arithmetic).
-template <typename R>
-__device__ __forceinline__ void elim_row(const Ops& o, double2 h3, double2 h2, double2 h1, double2 fe,
-                                         const typename Prec<R>::V* fq, typename Prec<R>::V* gp) {
-    const double2 mud = c2(fma(o.a1, h3.x + h1.x, o.a2 * h2.x), fma(o.a1, h3.y + h1.y, o.a2 * h2.y));
-    const R mx = (R)mud.x, my = (R)mud.y;
+// Plain and chosen form M u and the coupling in FP64; the fast form does the
+// whole row in FP32 as g = q ((M u) - (a1 + pole e) g_prev).
+template <int F>
+__device__ __forceinline__ void elim_row(const Ops& o, typename Form<F>::H h3, typename Form<F>::H h2,
+                                         typename Form<F>::H h1, typename Form<F>::E fe,
+                                         const typename Form<F>::V* fq, typename Form<F>::V* gp) {
+    using R = typename Form<F>::R;
+    if constexpr (F == kFast) {
+        const float mx = fmaf(o.a1f, h3.x + h1.x, o.a2f * h2.x), my = fmaf(o.a1f, h3.y + h1.y, o.a2f * h2.y);
 #pragma unroll
-    for (int t = 0; t < kT; ++t) {
-        // a1 + pole e cancels strongly for some terms: formed in FP64 like the
-        // factorisation, only al is rounded to the sweep precision
-        const double2 cin = caxpd(o.a1, o.pole[t], fe);
-        const double2 ci = cmul(cin, Prec<R>::up(fq[t]));
-        const R ax = (R)(-ci.x), ay = (R)(-ci.y);
-        const R tx = fma(fq[t].x, mx, -fq[t].y * my), ty = fma(fq[t].x, my, fq[t].y * mx);
-        typename Prec<R>::V g;
-        g.x = fma(ax, gp[t].x, fma(-ay, gp[t].y, tx));
-        g.y = fma(ax, gp[t].y, fma(ay, gp[t].x, ty));
-        gp[t] = g;
+        for (int t = 0; t < kT; ++t) {
+            // cin = a1 + pole e;  v = M u - cin g_prev;  g = q v
+            const float cx = o.a1f + fmaf(o.polef[t].x, fe.x, -o.polef[t].y * fe.y);
+            const float cy = fmaf(o.polef[t].x, fe.y, o.polef[t].y * fe.x);
+            const float vx = fmaf(-cx, gp[t].x, fmaf(cy, gp[t].y, mx));
+            const float vy = fmaf(-cx, gp[t].y, fmaf(-cy, gp[t].x, my));
+            float2 g;
+            g.x = fmaf(fq[t].x, vx, -fq[t].y * vy);
+            g.y = fmaf(fq[t].x, vy, fq[t].y * vx);
+            gp[t] = g;
+        }
+    } else {
+        const double2 mud = c2(fma(o.a1, h3.x + h1.x, o.a2 * h2.x), fma(o.a1, h3.y + h1.y, o.a2 * h2.y));
+        const R mx = (R)mud.x, my = (R)mud.y;
+#pragma unroll
+        for (int t = 0; t < kT; ++t) {
+            // a1 + pole e cancels strongly for some terms: formed in FP64 like the
+            // factorisation, only al is rounded to the sweep precision
+            const double2 cin = caxpd(o.a1, o.pole[t], fe);
+            const double2 ci = cmul(cin, Prec<R>::up(fq[t]));
+            const R ax = (R)(-ci.x), ay = (R)(-ci.y);
+            const R tx = fma(fq[t].x, mx, -fq[t].y * my), ty = fma(fq[t].x, my, fq[t].y * mx);
+            typename Prec<R>::V g;
+            g.x = fma(ax, gp[t].x, fma(-ay, gp[t].y, tx));
+            g.y = fma(ax, gp[t].y, fma(ay, gp[t].x, ty));
+            gp[t] = g;
+        }
     }
 }
 
 // One streamed row of a solve pass, in registers.
-template <typename R>
+template <int F>
 struct RowF {
-    using V = typename Prec<R>::V;
+    using V = typename Form<F>::V;
     double2 u;
-    double2 e;
+    typename Form<F>::E e;
     V w[kT], g[kT], q[kT];
 };
 
-template <typename R>
-__device__ __forceinline__ void load_row(const SumSmem& S, int slot, int lane, RowF<R>& f) {
-    using V = typename Prec<R>::V;
+template <int F>
+__device__ __forceinline__ void load_row(const SumSmem& S, int slot, int lane, RowF<F>& f) {
+    using V = typename Form<F>::V;
+    using E = typename Form<F>::E;
     f.u = S.q[slot][0][lane];
-    f.e = S.q[slot][1][lane];
+    f.e = *reinterpret_cast<const E*>(&S.q[slot][1][lane]);
 #pragma unroll
     for (int t = 0; t < kT; ++t) {
         f.w[t] = *reinterpret_cast<const V*>(&S.q[slot][2 + 3 * t][lane]);
@@ -313,29 +387,42 @@ __device__ __forceinline__ void load_row(const SumSmem& S, int slot, int lane, R
 }
 
 // Carried state of a solve pass.
-template <typename R>
+template <int F>
 struct SolveState {
-    using V = typename Prec<R>::V;
-    double2 h1, h2, h3;  // u_new of the last three rows (h1 newest)
-    V xp[kT];            // back-substitution chains
-    V gp[kT];            // elimination chains
+    using V = typename Form<F>::V;
+    typename Form<F>::H h1, h2, h3;  // u_new of the last three rows (h1 newest)
+    V xp[kT];                        // back-substitution chains
+    V gp[kT];                        // elimination chains
 };
+
+template <typename H>
+__device__ __forceinline__ H hsel(bool c, H a, H b) {
+    H r;
+    r.x = c ? a.x : b.x;
+    r.y = c ? a.y : b.y;
+    return r;
+}
 
 // Stream row r of a solve pass.  The elimination of row m = r -/+ 2 uses
 // (h3, h2, h1) = (u_{m-/+1}, u_m, u_{m+/-1}) and comes first; then the
 // back-substitution x_r = g_r - w_r x_{r-/+1} of each term and this lane's
-// share c_inf u_old (lane 0) + sum_t c_t x_t in FP64, and the exchange of
-// the ray's P shares, added in lane order (identical in every lane).
+// share c_inf u_old (lane 0) + sum_t c_t x_t (FP64; FP32 in the fast form),
+// and the exchange of the ray's P shares, added in lane order (identical in
+// every lane).
 // CHECK: rows outside a ray's column are handled with selects and predicated
 // stores (branch-free); without CHECK, r and m are interior rows of every
 // ray of the warp and r is no ray's first back-substitution row.
-template <typename R, int P, int PASS, bool DOWN, bool CHECK>
-__device__ __forceinline__ void solve_row(const PassPtrs<R>& p, const Lane& L, const Ops& o, const RowF<R>& f,
-                                          int r, SolveState<R>& st) {
-    using V = typename Prec<R>::V;
+template <int F, int P, int PASS, bool DOWN, bool CHECK>
+__device__ __forceinline__ void solve_row(const PassPtrs<F>& p, const Lane& L, const Ops& o, const RowF<F>& f,
+                                          int r, SolveState<F>& st) {
+    using R = typename Form<F>::R;
+    using V = typename Form<F>::V;
+    using H = typename Form<F>::H;
     const int nz = o.nz;
-    const double2 zero = c2(0.0, 0.0);
     const R zr = R(0);
+    H hzero;
+    hzero.x = 0;
+    hzero.y = 0;
     const bool valid = CHECK ? ((r >= 0) & (r <= nz + 1)) : true;
     const bool interior = CHECK ? ((r >= 1) & (r <= nz)) : true;
     if (PASS != kBackOnly) {
@@ -344,7 +431,7 @@ __device__ __forceinline__ void solve_row(const PassPtrs<R>& p, const Lane& L, c
         V g[kT];
 #pragma unroll
         for (int t = 0; t < kT; ++t) g[t] = st.gp[t];
-        elim_row<R>(o, st.h3, st.h2, st.h1, f.e, f.q, g);
+        elim_row<F>(o, st.h3, st.h2, st.h1, f.e, f.q, g);
         const int mo = (CHECK ? (mvalid ? m : 0) : m) * kTile;
 #pragma unroll
         for (int t = 0; t < kT; ++t) {
@@ -357,12 +444,19 @@ __device__ __forceinline__ void solve_row(const PassPtrs<R>& p, const Lane& L, c
             }
         }
     }
-    double2 un;
+    H un;
     if (PASS == kElimOnly) {
-        un = interior ? f.u : zero;
+        un = interior ? dn2<H>(f.u) : hzero;
     } else {
         const bool first = CHECK ? (DOWN ? (r == 1) : (r == nz)) : false;
-        double2 v = cmul(o.cinf, f.u);  // f.u is zero-filled except in lane 0
+        H v;
+        if constexpr (F == kFast) {
+            const float2 uf = dn2<float2>(f.u);  // zero-filled except in lane 0
+            v.x = fmaf(o.cinff.x, uf.x, -o.cinff.y * uf.y);
+            v.y = fmaf(o.cinff.x, uf.y, o.cinff.y * uf.x);
+        } else {
+            v = cmul(o.cinf, f.u);  // f.u is zero-filled except in lane 0
+        }
 #pragma unroll
         for (int t = 0; t < kT; ++t) {
             V x;
@@ -375,28 +469,34 @@ __device__ __forceinline__ void solve_row(const PassPtrs<R>& p, const Lane& L, c
                 x.y = interior ? x.y : zr;
             }
             st.xp[t] = x;
-            const double2 xd = Prec<R>::up(x);
-            v = c2(fma(o.ck[t].x, xd.x, fma(-o.ck[t].y, xd.y, v.x)), fma(o.ck[t].x, xd.y, fma(o.ck[t].y, xd.x, v.y)));
+            if constexpr (F == kFast) {
+                v.x = fmaf(o.ckf[t].x, x.x, fmaf(-o.ckf[t].y, x.y, v.x));
+                v.y = fmaf(o.ckf[t].x, x.y, fmaf(o.ckf[t].y, x.x, v.y));
+            } else {
+                const double2 xd = Prec<R>::up(x);
+                v = c2(fma(o.ck[t].x, xd.x, fma(-o.ck[t].y, xd.y, v.x)),
+                       fma(o.ck[t].x, xd.y, fma(o.ck[t].y, xd.x, v.y)));
+            }
         }
-        double2 sh[P];
+        H sh[P];
 #pragma unroll
         for (int j = 0; j < P; ++j) {
             sh[j].x = __shfl_sync(L.wmask, v.x, L.gbase + j);
             sh[j].y = __shfl_sync(L.wmask, v.y, L.gbase + j);
         }
-        double2 tot = sh[0];
+        H tot = sh[0];
 #pragma unroll
         for (int j = 1; j < P; ++j) {
             tot.x += sh[j].x;
             tot.y += sh[j].y;
         }
-        un = interior ? tot : zero;
-        if (interior & (L.k == 0)) p.u[(CHECK ? (interior ? r : 0) : r) * kTile] = un;
+        un = interior ? tot : hzero;
+        if (interior & (L.k == 0)) p.u[(CHECK ? (interior ? r : 0) : r) * kTile] = up2(un);
     }
     if (CHECK) {
-        st.h3 = valid ? st.h2 : st.h3;
-        st.h2 = valid ? st.h1 : st.h2;
-        st.h1 = valid ? un : st.h1;
+        st.h3 = hsel(valid, st.h2, st.h3);
+        st.h2 = hsel(valid, st.h1, st.h2);
+        st.h1 = hsel(valid, un, st.h1);
     } else {
         st.h3 = st.h2;
         st.h2 = st.h1;
@@ -405,20 +505,20 @@ __device__ __forceinline__ void solve_row(const PassPtrs<R>& p, const Lane& L, c
 }
 
 // Iterations [k0, k1) of a solve pass, kU rows each.
-template <typename R, int P, int PASS, bool DOWN, bool CHECK>
-__device__ __forceinline__ void solve_iters(const PassPtrs<R>& p, const Lane& L, SumSmem& S, const Ops& o, int k0,
-                                            int k1, SolveState<R>& st) {
+template <int F, int P, int PASS, bool DOWN, bool CHECK>
+__device__ __forceinline__ void solve_iters(const PassPtrs<F>& p, const Lane& L, SumSmem& S, const Ops& o, int k0,
+                                            int k1, SolveState<F>& st) {
 #pragma unroll 1
     for (int k = k0; k < k1; k += kU) {
         cp_wait<kSR - kU>();
-        RowF<R> f[kU];
+        RowF<F> f[kU];
 #pragma unroll
-        for (int j = 0; j < kU; ++j) load_row<R>(S, (k + j) & (kSR - 1), L.lane, f[j]);
+        for (int j = 0; j < kU; ++j) load_row<F>(S, (k + j) & (kSR - 1), L.lane, f[j]);
 #pragma unroll
         for (int j = 0; j < kU; ++j)
-            solve_issue<R, PASS, DOWN, CHECK>(p, L, S, (k + j) & (kSR - 1), row_of<DOWN>(L, k + j + kSR), o.nz);
+            solve_issue<F, PASS, DOWN, CHECK>(p, L, S, (k + j) & (kSR - 1), row_of<DOWN>(L, k + j + kSR), o.nz);
 #pragma unroll
-        for (int j = 0; j < kU; ++j) solve_row<R, P, PASS, DOWN, CHECK>(p, L, o, f[j], row_of<DOWN>(L, k + j), st);
+        for (int j = 0; j < kU; ++j) solve_row<F, P, PASS, DOWN, CHECK>(p, L, o, f[j], row_of<DOWN>(L, k + j), st);
     }
 }
 
@@ -427,20 +527,23 @@ __device__ __forceinline__ void solve_iters(const PassPtrs<R>& p, const Lane& L,
 // by lane 0 of the ray), eliminate the next solves.  kBackOnly:
 // back-substitute and combine only.  Rows are streamed in the pass
 // direction, kU per iteration.
-template <typename R, int P, int PASS, bool DOWN>
+template <int F, int P, int PASS, bool DOWN>
 __device__ void sum_pass(const SumArgs& a, const Lane& L, SumSmem& S, const Ops& o) {
+    using V = typename Form<F>::V;
+    using H = typename Form<F>::H;
     const int nz = o.nz;
-    const PassPtrs<R> p = pass_ptrs<R, DOWN>(a, L);
+    const PassPtrs<F> p = pass_ptrs<F, DOWN>(a, L);
     __threadfence_block();
     __syncwarp(L.wmask);
 #pragma unroll 1
-    for (int k = 0; k < kSR; ++k) solve_issue<R, PASS, DOWN, true>(p, L, S, k, row_of<DOWN>(L, k), nz);
-    SolveState<R> st;
-    st.h1 = st.h2 = st.h3 = c2(0.0, 0.0);
+    for (int k = 0; k < kSR; ++k) solve_issue<F, PASS, DOWN, true>(p, L, S, k, row_of<DOWN>(L, k), nz);
+    SolveState<F> st;
+    st.h1.x = st.h1.y = 0;
+    st.h2 = st.h3 = st.h1;
 #pragma unroll
     for (int t = 0; t < kT; ++t) {
-        st.xp[t] = {R(0), R(0)};
-        st.gp[t] = {R(0), R(0)};
+        st.xp[t].x = st.xp[t].y = 0;
+        st.gp[t].x = st.gp[t].y = 0;
     }
     // Iterations whose rows r (and elimination rows, and the rows they
     // prefetch) are interior rows of every ray of the warp, and past every
@@ -450,21 +553,21 @@ __device__ void sum_pass(const SumArgs& a, const Lane& L, SumSmem& S, const Ops&
     const int ub = DOWN ? L.nzmin + 2 - kSR - kU : L.span - kU - kSR;  // last steady start
     const int k_lo = min(L.span, (max(lb, 0) + kU - 1) / kU * kU);
     const int k_hi = ub < k_lo ? k_lo : min(L.span, (ub / kU) * kU + kU);
-    solve_iters<R, P, PASS, DOWN, true>(p, L, S, o, 0, k_lo, st);
-    solve_iters<R, P, PASS, DOWN, false>(p, L, S, o, k_lo, k_hi, st);
-    solve_iters<R, P, PASS, DOWN, true>(p, L, S, o, k_hi, L.span, st);
+    solve_iters<F, P, PASS, DOWN, true>(p, L, S, o, 0, k_lo, st);
+    solve_iters<F, P, PASS, DOWN, false>(p, L, S, o, k_lo, k_hi, st);
+    solve_iters<F, P, PASS, DOWN, true>(p, L, S, o, k_hi, L.span, st);
     // The last row to eliminate (m = nz DOWN, m = 1 UP) would need stream row
     // nz+2 / -1; its window (u_{m-1}, u_m, u_{m+1}) is already in the history.
     if (PASS != kBackOnly) {
-        using V = typename Prec<R>::V;
         const int m = DOWN ? nz : 1;
         V fq[kT];
 #pragma unroll
         for (int t = 0; t < kT; ++t) fq[t] = p.q[t][m * kTile];
-        elim_row<R>(o, st.h3, st.h2, st.h1, p.e[m * kTile], fq, st.gp);
+        elim_row<F>(o, st.h3, st.h2, st.h1, p.e[m * kTile], fq, st.gp);
 #pragma unroll
         for (int t = 0; t < kT; ++t) p.g[t][m * kTile] = st.gp[t];
     }
+    (void)sizeof(H);
     cp_wait<0>();
     __threadfence_block();
     __syncwarp(L.wmask);
@@ -510,21 +613,24 @@ __device__ void set_ops(const SumArgs& a, int rid, int set, const Lane& L, Ops* 
         // slots without a term solve a copy of term 0 with weight 0
         o->pole[t] = a.pd2[base + (j < n ? j : 0)];
         o->ck[t] = j < n ? a.pfc[base + j] : c2(0.0, 0.0);
+        o->polef[t] = dn2<float2>(o->pole[t]);
+        o->ckf[t] = dn2<float2>(o->ck[t]);
     }
     o->cinf = a.pfcinf[(long long)rid * kSets + set];
+    o->cinff = dn2<float2>(o->cinf);
 }
 
-template <typename R>
+template <int F>
 __device__ void sum_refactor(const SumArgs& a, const Lane& L, SumSmem& S, const Ops& o) {
-    sum_factor<R, true>(a, L, S, o);
-    sum_factor<R, false>(a, L, S, o);
+    sum_factor<F, true>(a, L, S, o);
+    sum_factor<F, false>(a, L, S, o);
     __threadfence_block();
     __syncwarp(L.wmask);
 }
 
 }  // namespace
 
-template <typename R, int P>
+template <int F, int P>
 __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SumSmem& S = *reinterpret_cast<SumSmem*>(smem_raw);
@@ -556,6 +662,8 @@ __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
     o.cfact = 0.5 / (ry.dz * ry.dz);
     o.a1 = ry.k0 * ry.k0 / 6.0;
     o.a2 = 2.0 * ry.k0 * ry.k0 / 3.0;
+    o.a1f = (float)o.a1;
+    o.a2f = (float)o.a2;
 
     // initial profiles, split over the ray's lanes (cupyram.py:571-608, profl)
     int iz = max(1, min(nz - 1, (int)floor(e.zb[0] / ry.dz)));
@@ -612,26 +720,26 @@ __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
     } while (0)
 #define CR_BACK_ONLY()                                                      \
     do {                                                                    \
-        if (pend_down) sum_pass<R, P, kBackOnly, false>(a, L, S, o);        \
-        else sum_pass<R, P, kBackOnly, true>(a, L, S, o);                   \
+        if (pend_down) sum_pass<F, P, kBackOnly, false>(a, L, S, o);        \
+        else sum_pass<F, P, kBackOnly, true>(a, L, S, o);                   \
         CR_FINISH_PENDING();                                                \
     } while (0)
 
     // self-starter: two steps of 1/(1-X), one of the ip=2 operator
     set_ops(a, rid, 0, L, &o);
-    sum_refactor<R>(a, L, S, o);
-    sum_pass<R, P, kElimOnly, true>(a, L, S, o);
+    sum_refactor<F>(a, L, S, o);
+    sum_pass<F, P, kElimOnly, true>(a, L, S, o);
     pend_down = true;
     pend_valid = true;
     pend_out = false;
-    sum_pass<R, P, kFusedP, false>(a, L, S, o);  // back-substitute step 1, eliminate step 2 (UP)
+    sum_pass<F, P, kFusedP, false>(a, L, S, o);  // back-substitute step 1, eliminate step 2 (UP)
     CR_FINISH_PENDING();
     pend_down = false;
     pend_valid = true;
     CR_BACK_ONLY();
     set_ops(a, rid, 1, L, &o);
-    sum_refactor<R>(a, L, S, o);
-    sum_pass<R, P, kElimOnly, true>(a, L, S, o);
+    sum_refactor<F>(a, L, S, o);
+    sum_pass<F, P, kElimOnly, true>(a, L, S, o);
     pend_down = true;
     pend_valid = true;
     pend_out = true;
@@ -689,18 +797,18 @@ __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
                 iz = iz_new;
                 set = new_set;
                 set_ops(a, rid, set, L, &o);
-                sum_factor<R, true>(a, L, S, o);
-                sum_factor<R, false>(a, L, S, o);
+                sum_factor<F, true>(a, L, S, o);
+                sum_factor<F, false>(a, L, S, o);
                 __threadfence_block();
             }
             __syncwarp(L.wmask);
-            sum_pass<R, P, kElimOnly, true>(a, L, S, o);
+            sum_pass<F, P, kElimOnly, true>(a, L, S, o);
             pend_down = true;
             first_march = false;
         } else {
             // back-substitute the pending step and eliminate this one in one pass
-            if (pend_down) sum_pass<R, P, kFusedP, false>(a, L, S, o);
-            else sum_pass<R, P, kFusedP, true>(a, L, S, o);
+            if (pend_down) sum_pass<F, P, kFusedP, false>(a, L, S, o);
+            else sum_pass<F, P, kFusedP, true>(a, L, S, o);
             CR_FINISH_PENDING();
             pend_down = !pend_down;
         }
@@ -716,26 +824,26 @@ __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
 #undef CR_FINISH_PENDING
 #undef CR_BACK_ONLY
 
-template <typename R, int P>
+template <int F, int P>
 static cudaError_t launch_one(const SumArgs& a, int count, cudaStream_t st) {
     const size_t smem = sizeof(SumSmem);
-    cudaError_t ce = cudaFuncSetAttribute(march_sum_kernel<R, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t ce = cudaFuncSetAttribute(march_sum_kernel<F, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (ce != cudaSuccess) return ce;
-    march_sum_kernel<R, P><<<count, kTile, smem, st>>>(a);
+    march_sum_kernel<F, P><<<count, kTile, smem, st>>>(a);
     return cudaGetLastError();
 }
 
-template <typename R, int P = 1>
+template <int F, int P = 1>
 static cudaError_t launch_p(const SumArgs& a, int p, int count, cudaStream_t st) {
     if constexpr (P > kMaxP) {
         return cudaErrorInvalidValue;
     } else {
-        if (p == P) return launch_one<R, P>(a, count, st);
-        return launch_p<R, P + 1>(a, p, count, st);
+        if (p == P) return launch_one<F, P>(a, count, st);
+        return launch_p<F, P + 1>(a, p, count, st);
     }
 }
 
-cudaError_t launch_march_sum(const SumArgs& a0, const int* tile_P, int n_tiles, int chosen,
+cudaError_t launch_march_sum(const SumArgs& a0, const int* tile_P, int n_tiles, int form,
                              const cudaStream_t* streams, int n_streams, int* launches) {
     // tiles are ordered by lanes per ray; one launch per run of equal P
     int begin = 0;
@@ -746,8 +854,9 @@ cudaError_t launch_march_sum(const SumArgs& a0, const int* tile_P, int n_tiles, 
         SumArgs a = a0;
         a.tile_begin = begin;
         const cudaStream_t st = streams[*launches % n_streams];
-        const cudaError_t ce = chosen ? launch_p<float>(a, tile_P[begin], end - begin, st)
-                                      : launch_p<double>(a, tile_P[begin], end - begin, st);
+        const cudaError_t ce = form == CR_CHOSEN_C64 ? launch_p<kFast>(a, tile_P[begin], end - begin, st)
+                               : form == CR_CHOSEN_C64R ? launch_p<kChosen>(a, tile_P[begin], end - begin, st)
+                                                        : launch_p<kPlain>(a, tile_P[begin], end - begin, st);
         if (ce != cudaSuccess) return ce;
         ++*launches;
         begin = end;

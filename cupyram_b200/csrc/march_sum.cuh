@@ -44,14 +44,17 @@ struct SumArgs {
     int tile_begin;             // first tile of this launch
 };
 
-// chosen = 1: complex64 factors / workspace, FP32 sweeps (the buffers given
-// for G and the factors are then read as float2).
+// form: an enum cr_precision value.  CR_PLAIN_C128: complex128 factors /
+// workspace and FP64 sweeps; CR_CHOSEN_C64R: complex64 factors / workspace
+// and FP32 sweeps (the buffers given for G and the factors are then read as
+// float2), terms combined in FP64; CR_CHOSEN_C64: as CR_CHOSEN_C64R with the
+// couplings (ED / EU read as float2), M u and the term combination in FP32.
 // Largest lanes-per-ray value the kernels are instantiated for (np <= 10).
 constexpr int kMaxP = (10 + kT - 1) / kT;
 // tile_P: host copy of tile_G.  One launch per run of equal P: run i goes
 // on streams[i % n_streams] (independent runs overlap); the number of
 // launches is returned in *launches.
-cudaError_t launch_march_sum(const SumArgs& a, const int* tile_P, int n_tiles, int chosen,
+cudaError_t launch_march_sum(const SumArgs& a, const int* tile_P, int n_tiles, int form,
                              const cudaStream_t* streams, int n_streams, int* launches);
 
 }  // namespace crk

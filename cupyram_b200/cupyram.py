@@ -8,9 +8,11 @@ this class only normalises, validates and reshapes on the host.
 
 Extra keyword arguments (not in the reference):
 
-``precision``  ``"plain"`` (complex128, default) or ``"chosen"`` (complex64
+``precision``  ``"plain"`` (complex128, default), ``"chosen"`` (complex64
                sweeps in FP32 arithmetic; the Pade terms are combined in FP64
-               and the field is kept in complex128).
+               and the field is kept in complex128) or ``"fast"`` (complex64
+               sweeps with an FP32 inner loop: couplings, M u and the term
+               combination in FP32 too).
 ``per_ray``    ``True`` pairs environment i with frequency i (no
                environment x frequency cross product) and gives every ray its
                own grid; ``zs``, ``zr``, ``dr``, ``dz``, ``np``, ``rmax`` may
@@ -32,7 +34,7 @@ import time
 import numpy as np
 
 from . import batch as _batch
-from .engine import Engine
+from .engine import PRECISIONS, Engine
 
 
 class CuPyRAM:
@@ -50,8 +52,8 @@ class CuPyRAM:
         self._compute_grids = bool(kwargs.get("compute_grids", True))
         self._max_workers = kwargs.get("max_workers", 8)
         self._precision = kwargs.get("precision", "plain")
-        if self._precision not in ("plain", "chosen"):
-            raise ValueError(f"precision must be 'plain' or 'chosen', got {self._precision!r}")
+        if self._precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}, got {self._precision!r}")
         self._benchmark_propagation = bool(kwargs.get("benchmark_propagation", False))
         envs, p, zs_env, zr_env, per_ray = _batch.prepare(
             freq, zs, zr, z_ss, rp_ss, cw, z_sb, rp_sb, cb, rhob, attn, rbzb, kwargs)

@@ -7,6 +7,12 @@ from . import _lib
 from .batch import Batch
 
 
+# precision forms of the march (enum cr_precision): "plain" complex128;
+# "chosen" complex64 sweeps with the terms combined in FP64; "fast" complex64
+# sweeps with an FP32 inner loop (couplings, M u and the combination in FP32)
+PRECISIONS = {"plain": _lib.CR_PLAIN_C128, "chosen": _lib.CR_CHOSEN_C64R, "fast": _lib.CR_CHOSEN_C64}
+
+
 class Engine:
     """Owns a cr_engine built from a packed :class:`Batch`.
 
@@ -20,9 +26,9 @@ class Engine:
     def __init__(self, batch: Batch, precision="plain"):
         self.lib = _lib.load()
         self.batch = batch
-        prec = {"plain": _lib.CR_PLAIN_C128, "chosen": _lib.CR_CHOSEN_C64R}.get(precision)
+        prec = PRECISIONS.get(precision)
         if prec is None:
-            raise ValueError(f"precision must be 'plain' or 'chosen', got {precision!r}")
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}, got {precision!r}")
         self._keep = (np.ascontiguousarray(batch.rays), np.ascontiguousarray(batch.envs),
                       np.ascontiguousarray(batch.pool, dtype=np.float64))
         rays, envs, pool = self._keep
@@ -148,11 +154,31 @@ def march_static(batch: Batch, dev_out, stream=0):
     desc.compute_grids = 1 if batch.compute_grids else 0
     desc.line_len, desc.grid_len = batch.line_len, batch.grid_len
 
+    need = {"tll": batch.line_len, "cpl": batch.line_len}
+    if batch.compute_grids:
+        need.update(tlg=batch.grid_len, cpg=batch.grid_len)
+    kinds = {"tll": "float64", "tlg": "float64", "cpl": "complex128", "cpg": "complex128"}
+
     def ptr(name):
         a = dev_out.get(name)
         if a is None:
+            if name in need:
+                raise ValueError(f"march_static: dev_out[{name!r}] is required")
             return None
-        return int(a) if isinstance(a, int) else int(a.data_ptr())
+        if isinstance(a, int):
+            return a  # a raw device address: the caller vouches for its size and type
+        # a tensor-like buffer: the kernel writes need[name] elements of the given type into it
+        dt = str(getattr(a, "dtype", "")).replace("torch.", "")
+        if dt != kinds[name]:
+            raise ValueError(f"march_static: dev_out[{name!r}] must be {kinds[name]}, got {dt or type(a).__name__}")
+        if not getattr(a, "is_cuda", False):
+            raise ValueError(f"march_static: dev_out[{name!r}] must be in device memory")
+        if hasattr(a, "is_contiguous") and not a.is_contiguous():
+            raise ValueError(f"march_static: dev_out[{name!r}] must be contiguous")
+        n = int(a.numel()) if hasattr(a, "numel") else int(a.size)
+        if name in need and n < need[name]:
+            raise ValueError(f"march_static: dev_out[{name!r}] holds {n} elements, the batch writes {need[name]}")
+        return int(a.data_ptr())
 
     o = _lib.CrOutputs(ptr("tll"), ptr("cpl"), ptr("tlg"), ptr("cpg"))
     _lib.check(lib.cr_march_static(ctypes.byref(desc), ctypes.byref(o), ctypes.c_void_p(stream or None)))

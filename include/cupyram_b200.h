@@ -46,9 +46,13 @@ enum cr_status {
 /* Arithmetic form of the range march. */
 enum cr_precision {
     CR_PLAIN_C128 = 0,   /* complex128 field and sweeps, FP64 arithmetic          */
-    CR_CHOSEN_C64R = 1   /* complex64 factors, workspace and sweeps (FP32 arithmetic);
+    CR_CHOSEN_C64R = 1,  /* complex64 factors, workspace and sweeps (FP32 arithmetic);
                             the Pade terms are combined in FP64 and the field is
                             kept in complex128                                    */
+    CR_CHOSEN_C64 = 2    /* complex64 factors and workspace with an FP32 inner loop:
+                            sweeps, couplings, M u and the term combination in
+                            FP32; the factorisation and the stored field stay
+                            FP64 / complex128                                     */
 };
 
 /*
@@ -146,9 +150,29 @@ int cr_pade(double freq, double c0, int np, int ns, double dr, int ip,
             double* pd1, double* pd2);
 
 /*
+ * Pade coefficients of n independent (freq, c0, np, ns, dr, ip) jobs, solved
+ * on the current CUDA device, one thread per job, by the same FP64
+ * construction as cr_pade.  Replaces the host loops that call
+ * compute_pade_coefficients once per environment and frequency
+ * (cupyram/cupyram.py:706-726, :984-999, :1040-1060) and the unused
+ * cupyram/pade.py:276-317 compute_pade_coefficients_batch.
+ *   freq, c0, dr: [n] doubles; np, ns, ip: [n] int32 (np 1..CR_MAX_NP,
+ *   ns 0..2, ip 1 or 2).  Host memory.
+ *   pd1, pd2: [n][CR_MAX_NP] complex (2*CR_MAX_NP doubles per job,
+ *   interleaved; zeros past the job's np).  status: [n] int32, CR_OK,
+ *   CR_EPADE (Laguerre did not converge) or CR_EINVAL per job.
+ * Returns CR_OK when every job succeeded, else the first failing job's code
+ * (its index in cr_global_error); CR_EINVAL for bad arguments, CR_ECUDA /
+ * CR_ENOMEM for device failures.  Synchronous; uses temporary device memory.
+ */
+int cr_pade_batch(int n, const double* freq, const double* c0, const int32_t* np,
+                  const int32_t* ns, const double* dr, const int32_t* ip,
+                  double* pd1, double* pd2, int32_t* status);
+
+/*
  * Build an engine for a batch: validates the description, computes the Pade
  * sets of every ray (self-starter, march, march without stability
- * constraints) on the host in FP64, sorts rays into device tiles by work and
+ * constraints) on the device in FP64 (as cr_pade_batch), sorts rays into device tiles by work and
  * allocates device memory.  Replaces the set-up half of CuPyRAM.run
  * (cupyram/cupyram.py:528-726: setup, profl, Pade batch).
  */
@@ -197,6 +221,17 @@ int cr_global_error(char* buf, size_t len);
 void cr_destroy(cr_engine* e);
 
 /*
+ * Engines take their device memory from a stream-ordered pool per device that
+ * keeps freed memory for the next engine, so that creating an engine per
+ * batch (as CuPyRAM.run() does for every call) costs no fresh cudaMalloc /
+ * cudaFree after the first.  CuPy's default memory pool plays this part for
+ * the reference; cr_release_cache returns the pooled memory that no live
+ * engine holds to the device, as cupyram/benchmark.py:35-36 does with
+ * get_default_memory_pool().free_all_blocks().
+ */
+int cr_release_cache(void);
+
+/*
  * Size in bytes of the device scratch built into the library for
  * cr_march_static (a file-scope device array; every GPU that loads the
  * library holds it until the process exits).
@@ -235,7 +270,10 @@ void cr_destroy(cr_engine* e);
  * current: it looks up the scratch array's device address
  * (cudaGetSymbolAddress), and the driver loads the library's kernels and
  * their fixed local memory.  Make that first call during the caller's own
- * initialisation, before any stream capture.  Every call shares the one scratch array and
+ * initialisation, before any stream capture.  The address is kept with the
+ * handle of the context it was looked up in; a call in a new context of the
+ * device (after cudaDeviceReset, say) repeats the look-up, so no call uses an
+ * address of a context that no longer exists.  Every call shares the one scratch array and
  * it keeps the last call's contents (everything a march needs is rewritten
  * or cleared by the call itself), so calls whose work overlaps on the GPU -
  * from two threads, or on two streams of one device - race and must be

@@ -127,7 +127,7 @@ def test_header_constants_match_the_binding():
     assert int(np.prod([int(x) for x in defines["CR_STATIC_SCRATCH_BYTES"].split("*")])) == _lib.STATIC_SCRATCH_BYTES
     enums = {k: int(v) for k, v in re.findall(r"\b(CR_[A-Z0-9_]+)\s*=\s*(\d+)", text)}
     for name in ("CR_OK", "CR_EINVAL", "CR_ECUDA", "CR_EPADE", "CR_ETIMEOUT", "CR_ENAN", "CR_ENOMEM", "CR_ESTATE",
-                 "CR_PLAIN_C128", "CR_CHOSEN_C64R"):
+                 "CR_PLAIN_C128", "CR_CHOSEN_C64R", "CR_CHOSEN_C64"):
         assert enums[name] == getattr(_lib, name), name
 
 

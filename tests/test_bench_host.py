@@ -55,3 +55,21 @@ def test_clock_sampler_reads_a_running_sampler(tmp_path, monkeypatch):
     c = clk.summary()
     assert c["samples"] >= 3 and c["sm_mhz"] == 1800.0 and c["reasons"] == ["sw_power_cap"]
     assert not os.path.exists(path)
+
+
+def test_sample_parity_compares_only_the_sampled_rays():
+    """The bench's parity record: TL-line differences of the sampled rays, in
+    their ragged layout, and nothing of the other rays."""
+    from types import SimpleNamespace
+    rays = np.zeros(3, dtype=[("line_off", "i8"), ("nvr", "i4")])
+    rays["line_off"] = [0, 4, 9]
+    rays["nvr"] = [4, 5, 2]
+    batch = SimpleNamespace(rays=rays)
+    tll = np.arange(11, dtype=np.float64)
+    ref = {"tll": tll.copy()}
+    ref["tll"][5] += 0.002  # ray 1
+    ref["tll"][10] += 5.0   # ray 2: not sampled
+    p = bench.sample_parity(batch, np.array([0, 1]), ref, tll)
+    assert p["rays"] == 2 and p["outputs"] == 9
+    assert abs(p["max_db"] - 0.002) < 1e-12
+    assert abs(p["rms_db"] - np.sqrt(0.002 ** 2 / 9)) < 1e-12

@@ -71,3 +71,48 @@ def test_static_rejects_batch_beyond_scratch(cuda_device):
     out = _device_outputs(torch, b)
     with pytest.raises(ValueError, match="scratch"):
         march_static(b, out)
+
+
+def _failing_pade_batch():
+    """pekeris_small with np 10 and dr 0.9077 m at 50 Hz, c0 1500 m/s: the
+    self-starter's Pade set (ip 2, ns 1) does not converge in the Laguerre
+    root search (the host path raises the same error)."""
+    args, kw, _ = load_case("pekeris_small")
+    envs, p, zs, zr, pr = B.prepare(*args, dict(kw, np=10, dr=0.9076932507005218, rmax=200.0))
+    return B.build_batch(envs, p, zs, zr, pr, False)
+
+
+def test_static_reports_pade_failure_every_call(cuda_device):
+    """A Pade set that fails on the device is reported on every call, never
+    cleared by the other rays' set-up threads, and a valid batch afterwards
+    still matches the allocating path."""
+    import torch
+    bad = _failing_pade_batch()
+    with pytest.raises(ValueError, match="Laguerre"):
+        Engine(bad)  # the host path refuses the same set
+    for call in range(4):
+        out = _device_outputs(torch, bad)
+        with pytest.raises(ValueError, match="Laguerre"):
+            march_static(bad, out, stream=torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+    good = _batch("pekeris_small", False)
+    with Engine(good) as eng:
+        ref = eng.run()
+    out = _device_outputs(torch, good)
+    march_static(good, out, stream=torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    n = good.line_len
+    assert np.abs(out["tll"].cpu().numpy()[:n] - ref["tll"][:n]).max() < TOL_DB
+
+
+def test_static_checks_output_buffers(cuda_device):
+    """Output tensors of the wrong type, place or size are refused before the call."""
+    import torch
+    b = _batch("pekeris_small", False)
+    out = _device_outputs(torch, b)
+    with pytest.raises(ValueError, match="float64"):
+        march_static(b, dict(out, tll=out["tll"].float()))
+    with pytest.raises(ValueError, match="device memory"):
+        march_static(b, dict(out, cpl=out["cpl"].cpu()))
+    with pytest.raises(ValueError, match="elements"):
+        march_static(b, dict(out, tll=out["tll"][: b.line_len - 1]))
