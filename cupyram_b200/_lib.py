@@ -13,7 +13,7 @@ import numpy as np
 LIB_NAME = "libcupyram_b200.so"
 LIB_PATH = Path(__file__).resolve().parent / LIB_NAME
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 MAX_NP = 10
 
 # status codes (enum cr_status)
@@ -53,7 +53,10 @@ class CrStats(ctypes.Structure):
                 ("d2h_bytes", ctypes.c_int64), ("kernel_launches", ctypes.c_int32),
                 ("rays_failed", ctypes.c_int32), ("tile_rays", ctypes.c_int32),
                 ("n_tiles", ctypes.c_int32), ("device_bytes", ctypes.c_int64),
-                ("column_rays", ctypes.c_int32), ("column_launches", ctypes.c_int32)]
+                ("column_rays", ctypes.c_int32), ("column_launches", ctypes.c_int32),
+                ("queue_ctas", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("create_ms", ctypes.c_double), ("pade_ms", ctypes.c_double),
+                ("tuner_row_step_s", ctypes.c_double), ("tuner_updates_per_s", ctypes.c_double)]
 
 
 # every symbol the header declares, with its signature
@@ -77,6 +80,8 @@ _SIGS = {
                                    ctypes.POINTER(ctypes.c_double)]),
     "cr_destroy": (None, [ctypes.c_void_p]),
     "cr_release_cache": (ctypes.c_int, []),
+    "cr_plan_columns": (ctypes.c_int, [ctypes.POINTER(CrBatch), ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_void_p]),
     "cr_march_static": (ctypes.c_int, [ctypes.POINTER(CrBatch), ctypes.POINTER(CrOutputs), ctypes.c_void_p]),
     "cr_cell_tl": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_void_p]),

@@ -36,6 +36,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -610,6 +611,12 @@ struct cr_engine {
     long long lane_elems = 0;
     std::vector<double2> pfc, pfcinf;
     int* d_tile_G = nullptr;
+    // device work queue of the batched march: tiles in longest-march-first
+    // order and the ticket counter the persistent launch takes them by
+    bool queue_mode = true;
+    std::vector<int> queue;
+    int* d_queue = nullptr;
+    int* d_ticket = nullptr;
     long long* d_tile_off = nullptr;
     long long* d_tile_loff = nullptr;
     double2 *d_pfc = nullptr, *d_pfcinf = nullptr;
@@ -699,7 +706,8 @@ void free_all(cr_engine* e) {
                     e->d_f1,   e->d_f2,   e->d_f3,   e->d_ksq,      e->d_u,   e->d_W,   e->d_G,
                     e->d_tll,  e->d_cpl,  e->d_tlg,  e->d_cpg,      e->d_flags, e->d_S1, e->d_S2,
                     e->d_S3,   e->d_AL,   e->d_WF,   e->d_tile_G,  e->d_tile_off, e->d_tile_loff, e->d_pfc, e->d_pfcinf,
-                    e->d_QD,   e->d_WD,   e->d_QU,   e->d_WU,      e->d_ED,  e->d_EU, e->d_col_ray};
+                    e->d_QD,   e->d_WD,   e->d_QU,   e->d_WU,      e->d_ED,  e->d_EU, e->d_col_ray,
+                    e->d_queue, e->d_ticket};
     // stream-ordered frees on the engine's stream (every other stream of the
     // engine joins it at the end of each march), back into the pool
     if (e->stream) {
@@ -1174,35 +1182,61 @@ double operator_changes(const cr_batch* b, const cr_ray& r) {
     return std::min(excursion / r.dz, (double)r.nr) + (double)(v.n_rss - 1) + (double)(v.n_rsb - 1);
 }
 
-// Rays marched by the column-parallel kernel instead of the batched one.
-// A ray's lockstep march in a batched tile takes about (nz + 2)(nr + 4)
-// row steps of one warp in sequence; when that alone exceeds the time the
-// whole batch needs at the batched kernel's throughput by a margin, the ray
-// would set the launch's length, and a cluster of SMs marches it instead.  A ray must
-// fit the shared memory of a cluster of at most 16 CTAs.  CUPYRAM_B200_COL:
-// 0 never, 1 every ray that fits, unset / other: this rule.
-std::vector<char> pick_column_rays(const cr_batch* b, const std::vector<int>& pd_n, bool chosen) {
-    constexpr double kRowStepSeconds = 0.3e-6;    // batched tile, one row of one step
-    constexpr double kUpdatesPerSecond = 1.3e10;  // batched kernel, whole GPU
+// Costs of the batched march that the column policy weighs, measured on the
+// device by the engine's own tuner (march_costs) unless given explicitly.
+struct MarchCosts {
+    double row_step_s = 0.0;     // one batched tile alone: one row of one step
+    double updates_per_s = 0.0;  // batched kernel over a device-filling batch
+};
+
+// The cost rule of the column policy.  A ray's lockstep march in a batched
+// tile takes about (nz + 2)(nr + 4 + 4 x operator changes) row steps of one
+// warp in sequence; when that alone exceeds the time the whole batch needs at
+// the batched kernel's throughput by the margin, the ray would set the
+// launch's length, and a cluster of SMs marches it instead.
+std::vector<char> cost_rule(const cr_batch* b, const MarchCosts& c) {
     // a ray leaves the batched kernel only when it would clearly outlast the
     // batch: in a homogeneous batch every ray's march is close to the
     // balanced time, and the batched kernel is the efficient one there
     constexpr double kMargin = 1.25;
     std::vector<char> col((size_t)b->n_rays, 0);
-    const char* env = getenv("CUPYRAM_B200_COL");
-    const int mode = (env && env[0] == '0') ? 0 : ((env && env[0] == '1') ? 1 : 2);
-    if (mode == 0) return col;
     double work = 0.0;
     for (int i = 0; i < b->n_rays; ++i) work += (double)b->rays[i].nz * b->rays[i].nr;
-    const double tau = work / kUpdatesPerSecond;
-    std::map<std::tuple<int, int, int>, bool> runs;
+    const double tau = work / c.updates_per_s;
     for (int i = 0; i < b->n_rays; ++i) {
         const cr_ray& r = b->rays[i];
         // every operator change (bathymetry index, profile update) costs the
         // batched march about four more passes: back-substitution alone, two
         // factorisation passes, elimination alone
         const double steps = (double)(r.nr + 4) + 4.0 * operator_changes(b, r);
-        if (mode == 2 && (double)(r.nz + 2) * steps * kRowStepSeconds <= kMargin * tau) continue;
+        col[(size_t)i] = (double)(r.nz + 2) * steps * c.row_step_s > kMargin * tau;
+    }
+    return col;
+}
+
+MarchCosts march_costs(int device, int precision);
+thread_local bool g_in_tuner = false;  // set while the tuner's own batches are created
+
+// Rays marched by the column-parallel kernel instead of the batched one: the
+// cost rule with the tuner's measured costs, for rays that fit the shared
+// memory of a cluster of at most 16 CTAs.  CUPYRAM_B200_COL: 0 never, 1 every
+// ray that fits, unset / other: the cost rule.
+std::vector<char> pick_column_rays(const cr_batch* b, const std::vector<int>& pd_n, int precision, int device,
+                                   MarchCosts* used) {
+    const bool chosen = precision != CR_PLAIN_C128;
+    std::vector<char> col((size_t)b->n_rays, 0);
+    const char* env = getenv("CUPYRAM_B200_COL");
+    const int mode = (env && env[0] == '0') ? 0 : ((env && env[0] == '1') ? 1 : 2);
+    if (mode == 0 || g_in_tuner) return col;
+    std::vector<char> want((size_t)b->n_rays, 1);
+    if (mode == 2) {
+        *used = march_costs(device, precision);
+        want = cost_rule(b, *used);
+    }
+    std::map<std::tuple<int, int, int>, bool> runs;
+    for (int i = 0; i < b->n_rays; ++i) {
+        if (!want[(size_t)i]) continue;
+        const cr_ray& r = b->rays[i];
         const int terms = col_terms(pd_n, i);
         const int cluster = crk::col_cluster_size(r.nz, terms, chosen);
         if (cluster == 0) continue;
@@ -1229,7 +1263,9 @@ int cr_create(const cr_batch* b, cr_engine** out) {
         set_global_error("cr_create: %s", msg.c_str());
         return CR_EINVAL;
     }
+    const auto t_create = std::chrono::steady_clock::now();
     cr_engine* e = new cr_engine();
+    cudaGetDevice(&e->device);  // a failure resurfaces at the first device call below
     e->n_rays = b->n_rays;
     e->n_envs = b->n_envs;
     e->precision = b->precision;
@@ -1237,7 +1273,9 @@ int cr_create(const cr_batch* b, cr_engine** out) {
     e->line_len = b->line_len;
     e->grid_len = b->compute_grids ? b->grid_len : 0;
     e->pool_len = b->pool_len;
+    const auto t_pade = std::chrono::steady_clock::now();
     int rc = compute_pade_sets(e, b);
+    e->st.pade_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_pade).count();
     if (rc) {
         set_global_error("%s", e->err.c_str());
         delete e;
@@ -1275,7 +1313,10 @@ int cr_create(const cr_batch* b, cr_engine** out) {
         return wx > wy;
     });
     if (e->sum_mode) {
-        const std::vector<char> is_col = pick_column_rays(b, e->pd_n, b->precision != CR_PLAIN_C128);
+        MarchCosts costs;
+        const std::vector<char> is_col = pick_column_rays(b, e->pd_n, b->precision, e->device, &costs);
+        e->st.tuner_row_step_s = costs.row_step_s;
+        e->st.tuner_updates_per_s = costs.updates_per_s;
         // batched rays grouped by Pade order, then work; a tile holds
         // floor(32/G) rays of G lanes each, G = the largest np in the tile
         std::vector<int> bord;
@@ -1304,6 +1345,7 @@ int cr_create(const cr_batch* b, cr_engine** out) {
         e->rays.resize(b->n_rays);
         long long off = 0;
         size_t pos = 0;
+        std::vector<double> tile_work;  // lockstep row-steps of each tile
         while (pos < bord.size()) {
             // lanes per ray: each lane carries kT terms of the tile's largest np
             const int G = (b->rays[bord[pos]].np + crk::kT - 1) / crk::kT;
@@ -1312,6 +1354,9 @@ int cr_create(const cr_batch* b, cr_engine** out) {
             int rows = 0;
             for (size_t q = pos; q < end; ++q) rows = std::max(rows, b->rays[bord[q]].nz + 2);
             const int t = (int)e->tile_G.size();
+            int nr_tile = 0;
+            for (size_t q = pos; q < end; ++q) nr_tile = std::max(nr_tile, b->rays[bord[q]].nr);
+            tile_work.push_back((double)rows * (double)(nr_tile + 4));
             e->tile_G.push_back(G);
             e->tile_off.push_back(off);
             e->tile_loff.push_back(e->lane_elems);
@@ -1331,6 +1376,15 @@ int cr_create(const cr_batch* b, cr_engine** out) {
             pos = end;
         }
         e->n_tiles = (int)e->tile_G.size();
+        // queue order: the longest lockstep marches first (ties: layout order)
+        e->queue.resize((size_t)e->n_tiles);
+        std::iota(e->queue.begin(), e->queue.end(), 0);
+        std::stable_sort(e->queue.begin(), e->queue.end(),
+                         [&](int x, int y) { return tile_work[(size_t)x] > tile_work[(size_t)y]; });
+        {
+            const char* qenv = getenv("CUPYRAM_B200_QUEUE");
+            e->queue_mode = !(qenv && qenv[0] == '0');
+        }
         e->term_capacity.assign((size_t)b->n_rays, 0);
         for (int t = 0; t < e->n_tiles; ++t)
             for (int l = 0; l < kTile; ++l) {
@@ -1472,6 +1526,8 @@ int cr_create(const cr_batch* b, cr_engine** out) {
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_EU, (size_t)e->col_elems);
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tile_loff, e->tile_loff.size());
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tile_G, e->tile_G.size());
+        if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_queue, e->queue.size());
+        if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_ticket, (size_t)1);
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tile_off, e->tile_off.size());
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_pfc, e->pfc.size());
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_pfcinf, e->pfcinf.size());
@@ -1520,6 +1576,7 @@ int cr_create(const cr_batch* b, cr_engine** out) {
     e->st.n_tiles = e->n_tiles;
     e->st.device_bytes = e->device_bytes;
     e->st.column_rays = (int)e->col_ray.size();
+    e->st.create_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_create).count();
     *out = e;
     return CR_OK;
 }
@@ -1565,6 +1622,7 @@ int cr_upload(cr_engine* e) {
     cp(e->d_pd_n, e->pd_n.data(), e->pd_n.size() * sizeof(int));
     if (e->sum_mode) {
         cp(e->d_tile_G, e->tile_G.data(), e->tile_G.size() * sizeof(int));
+        cp(e->d_queue, e->queue.data(), e->queue.size() * sizeof(int));
         cp(e->d_tile_off, e->tile_off.data(), e->tile_off.size() * sizeof(long long));
         cp(e->d_tile_loff, e->tile_loff.data(), e->tile_loff.size() * sizeof(long long));
         cp(e->d_pfc, e->pfc.data(), e->pfc.size() * sizeof(double2));
@@ -1683,10 +1741,23 @@ int cr_march(cr_engine* e) {
             ++nl;
         }
         sa.tile_begin = 0;
+        sa.ticket = e->d_ticket;
+        sa.queue = e->d_queue;
+        sa.n_queue = e->n_tiles;
         int nb = 0;
-        if (ce == cudaSuccess)
+        if (e->queue_mode) {
+            // one persistent launch over every batched tile, fed by the queue
+            int ctas = 0;
+            if (ce == cudaSuccess && e->n_tiles > 0) ce = cudaMemsetAsync(e->d_ticket, 0, sizeof(int), e->stream);
+            if (ce == cudaSuccess && e->n_tiles > 0) {
+                ce = crk::launch_march_sum_queue(sa, e->n_tiles, e->precision, e->stream, &ctas);
+                nb = 1;
+            }
+            e->st.queue_ctas = ctas;
+        } else if (ce == cudaSuccess) {
             ce = crk::launch_march_sum(sa, e->tile_G.data(), e->n_tiles, e->precision, e->sum_streams.data(),
                                        (int)e->sum_streams.size(), &nb);
+        }
         for (size_t i = 1; i < e->sum_streams.size(); ++i) {
             if (ce == cudaSuccess) ce = cudaEventRecord(e->sum_done[i], e->sum_streams[i]);
             if (ce == cudaSuccess) ce = cudaStreamWaitEvent(e->stream, e->sum_done[i], 0);
@@ -1839,6 +1910,137 @@ void cr_destroy(cr_engine* e) {
     free_all(e);
     delete e;
 }
+
+int cr_plan_columns(const cr_batch* b, double row_step_s, double updates_per_s, int32_t* is_column) {
+    const std::string msg = validate(b);
+    if (!msg.empty() || !is_column || !(row_step_s > 0.0) || !(updates_per_s > 0.0)) {
+        set_global_error("cr_plan_columns: %s", msg.empty() ? "invalid arguments" : msg.c_str());
+        return CR_EINVAL;
+    }
+    MarchCosts c;
+    c.row_step_s = row_step_s;
+    c.updates_per_s = updates_per_s;
+    const std::vector<char> col = cost_rule(b, c);
+    for (int i = 0; i < b->n_rays; ++i) is_column[i] = col[(size_t)i];
+    return CR_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// The engine's own tuner: the two costs of the column policy, measured once
+// per device and precision form by marching synthetic batches through the
+// engine itself (all rays on the batched kernel):
+//   * one tile alone (10 rays of np 6, nz 2000, 30 steps): the time of one
+//     row of one step of a lockstep tile, the latency-bound case;
+//   * two rounds of tiles for every resident slot of the device (nz 200,
+//     40 steps): the batched kernel's throughput in grid-point updates/s.
+// About 0.1 s on first use; CUPYRAM_B200_COSTS="row_step_s,updates_per_s"
+// sets both instead (reproducible schedules).
+std::mutex g_costs_mu;
+std::map<std::pair<int, int>, MarchCosts> g_costs;
+
+// Synthetic batch: isovelocity 100 m water over a 1700 m/s bottom, 100 Hz.
+struct SynthBatch {
+    std::vector<cr_ray> rays;
+    cr_env env{};
+    std::vector<double> pool;
+    cr_batch b{};
+};
+
+void synth_batch(SynthBatch& s, int n_rays, int nz, int nr, int precision) {
+    const double D = 100.0, c = 1500.0, rmax = 1.0e5;
+    const double dz = (D + 100.0) / (double)(nz + 1);
+    // z_ss, rp_ss, cw[1][2], z_sb, rp_sb, cb, rhob, attn [1][2], rb, zb
+    s.pool = {0.0, D, 0.0, c, c, D, D + 100.0, 0.0, 1700.0, 1700.0, 1.5, 1.5, 0.5, 0.5, 0.0, rmax, D, D};
+    s.env = cr_env{2, 1, 2, 1, 2, 0, 0};
+    s.rays.assign((size_t)n_rays, cr_ray{});
+    for (int i = 0; i < n_rays; ++i) {
+        cr_ray& r = s.rays[(size_t)i];
+        r.freq = 100.0;
+        r.c0 = c;
+        r.zs = r.zr = 20.0;
+        r.dz = dz;
+        r.dr = 5.0;
+        r.zmax = (double)(nz + 1) * dz;
+        r.lyrw_lambda = 0.0;
+        r.attnf = 10.0;
+        r.rs = INFINITY;
+        r.nz = nz;
+        r.nr = nr;
+        r.np = 6;
+        r.ns = 1;
+        r.ndr = 1;
+        r.ndz = 1;
+        r.nvr = 1;
+        r.nvz = 0;
+        r.env = 0;
+        r.line_off = i;
+        r.grid_off = -1;
+    }
+    s.b.n_rays = n_rays;
+    s.b.n_envs = 1;
+    s.b.rays = s.rays.data();
+    s.b.envs = &s.env;
+    s.b.pool = s.pool.data();
+    s.b.pool_len = (int64_t)s.pool.size();
+    s.b.precision = precision;
+    s.b.compute_grids = 0;
+    s.b.line_len = n_rays;
+    s.b.grid_len = 0;
+}
+
+// Device time (ms) of a warm march of a synthetic batch, or < 0 on failure.
+double synth_march_ms(int n_rays, int nz, int nr, int precision) {
+    SynthBatch s;
+    synth_batch(s, n_rays, nz, nr, precision);
+    cr_engine* e = nullptr;
+    if (cr_create(&s.b, &e) != CR_OK) return -1.0;
+    std::vector<double> tll((size_t)n_rays), cpl(2 * (size_t)n_rays);
+    cr_outputs o{tll.data(), cpl.data(), nullptr, nullptr};
+    double ms = -1.0;
+    if (cr_run(e, &o) == CR_OK && cr_march(e) == CR_OK) ms = e->st.march_ms;
+    cr_destroy(e);
+    return ms;
+}
+
+MarchCosts march_costs(int device, int precision) {
+    MarchCosts c;
+    if (const char* v = getenv("CUPYRAM_B200_COSTS")) {
+        if (sscanf(v, "%lf,%lf", &c.row_step_s, &c.updates_per_s) == 2 && c.row_step_s > 0 && c.updates_per_s > 0)
+            return c;
+    }
+    std::lock_guard<std::mutex> lock(g_costs_mu);
+    const auto key = std::make_pair(device, precision);
+    auto it = g_costs.find(key);
+    if (it != g_costs.end()) return it->second;
+    // if a measurement fails: one B200's figures for the plain form
+    c.row_step_s = 0.3e-6;
+    c.updates_per_s = 1.3e10;
+    g_in_tuner = true;
+    {
+        const int nz1 = 2000, nr1 = 30;
+        const double t1 = synth_march_ms(10, nz1, nr1, precision);
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        const int rays2 = 10 * 2 * 7 * sms, nz2 = 200, nr2 = 40;
+        const double t2 = synth_march_ms(rays2, nz2, nr2, precision);
+        // passes of a march without operator changes: about nr + 12 row sweeps
+        if (t1 > 0.0) c.row_step_s = t1 * 1e-3 / ((double)(nz1 + 2) * (double)(nr1 + 12));
+        if (t2 > 0.0) c.updates_per_s = (double)rays2 * nz2 * nr2 / (t2 * 1e-3);
+    }
+    g_in_tuner = false;
+    // the tuner's engines leave their memory in the pool: hand it back
+    cudaMemPool_t pool = nullptr;
+    if (engine_pool(device, &pool) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+    g_costs[key] = c;
+    return c;
+}
+
+}  // namespace
+
+extern "C" {
 
 int cr_release_cache(void) {
     std::lock_guard<std::mutex> lock(g_pool_mu);

@@ -37,6 +37,8 @@
 // golden cases it matches the product form to <= 5e-8 dB (oracle mode "sum").
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "march_common.cuh"
 #include "march_sum.cuh"
 
@@ -630,11 +632,10 @@ __device__ void sum_refactor(const SumArgs& a, const Lane& L, SumSmem& S, const 
 
 }  // namespace
 
+// The whole march of tile t (self-starter, every range step, the outputs) by
+// the calling warp; lanes without a ray return at once.
 template <int F, int P>
-__global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    SumSmem& S = *reinterpret_cast<SumSmem*>(smem_raw);
-    const int t = a.tile_begin + blockIdx.x;
+__device__ __forceinline__ void march_tile(const SumArgs& a, SumSmem& S, int t) {
     Lane L;
     L.lane = threadIdx.x;
     L.P = P;
@@ -824,6 +825,41 @@ __global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
 #undef CR_FINISH_PENDING
 #undef CR_BACK_ONLY
 
+// One tile per CTA (one launch per lanes-per-ray value P).
+template <int F, int P>
+__global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SumSmem& S = *reinterpret_cast<SumSmem*>(smem_raw);
+    march_tile<F, P>(a, S, a.tile_begin + blockIdx.x);
+}
+
+template <int F, int P = 1>
+__device__ __forceinline__ void march_tile_p(const SumArgs& a, SumSmem& S, int t, int p) {
+    if constexpr (P <= kMaxP) {
+        if (p == P) march_tile<F, P>(a, S, t);
+        else march_tile_p<F, P + 1>(a, S, t, p);
+    }
+}
+
+// Persistent march over every batched tile of the engine: each CTA (one
+// warp) takes the next tile from the device work queue - an atomic ticket
+// over a.queue, the tiles in longest-march-first order - until the queue is
+// empty, whatever its lanes per ray.  Taking a ticket never waits.
+template <int F>
+__global__ void __launch_bounds__(kTile) march_sum_queue_kernel(SumArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SumSmem& S = *reinterpret_cast<SumSmem*>(smem_raw);
+    for (;;) {
+        int k = 0;
+        if (threadIdx.x == 0) k = atomicAdd(a.ticket, 1);
+        k = __shfl_sync(0xffffffffu, k, 0);
+        if (k >= a.n_queue) break;
+        const int t = a.queue[k];
+        march_tile_p<F>(a, S, t, a.tile_G[t]);
+        __syncwarp();
+    }
+}
+
 template <int F, int P>
 static cudaError_t launch_one(const SumArgs& a, int count, cudaStream_t st) {
     const size_t smem = sizeof(SumSmem);
@@ -841,6 +877,31 @@ static cudaError_t launch_p(const SumArgs& a, int p, int count, cudaStream_t st)
         if (p == P) return launch_one<F, P>(a, count, st);
         return launch_p<F, P + 1>(a, p, count, st);
     }
+}
+
+template <int F>
+static cudaError_t launch_queue_f(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas) {
+    const size_t smem = sizeof(SumSmem);
+    cudaError_t ce = cudaFuncSetAttribute(march_sum_queue_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem);
+    if (ce != cudaSuccess) return ce;
+    int dev = 0, sms = 0, per_sm = 0;
+    ce = cudaGetDevice(&dev);
+    if (ce == cudaSuccess) ce = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (ce == cudaSuccess)
+        ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, march_sum_queue_kernel<F>, kTile, smem);
+    if (ce != cudaSuccess) return ce;
+    // every resident slot of the device, and no more CTAs than tiles
+    *ctas = std::max(1, std::min(n_tiles, std::max(1, per_sm) * sms));
+    march_sum_queue_kernel<F><<<*ctas, kTile, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_march_sum_queue(const SumArgs& a, int n_tiles, int form, cudaStream_t st, int* ctas) {
+    if (n_tiles <= 0) return cudaSuccess;
+    return form == CR_CHOSEN_C64 ? launch_queue_f<kFast>(a, n_tiles, st, ctas)
+           : form == CR_CHOSEN_C64R ? launch_queue_f<kChosen>(a, n_tiles, st, ctas)
+                                    : launch_queue_f<kPlain>(a, n_tiles, st, ctas);
 }
 
 cudaError_t launch_march_sum(const SumArgs& a0, const int* tile_P, int n_tiles, int form,

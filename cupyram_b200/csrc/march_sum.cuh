@@ -41,7 +41,12 @@ struct SumArgs {
     double2* cpg;
     int* flags;
     int compute_grids;
-    int tile_begin;             // first tile of this launch
+    int tile_begin;             // first tile of this launch (one launch per P)
+    // device work queue of the persistent launch: ticket counter (zero at
+    // launch), and the n_queue tiles in the order they are taken
+    int* ticket;
+    const int* queue;
+    int n_queue;
 };
 
 // form: an enum cr_precision value.  CR_PLAIN_C128: complex128 factors /
@@ -54,6 +59,12 @@ constexpr int kMaxP = (10 + kT - 1) / kT;
 // tile_P: host copy of tile_G.  One launch per run of equal P: run i goes
 // on streams[i % n_streams] (independent runs overlap); the number of
 // launches is returned in *launches.
+// One persistent launch over all n_tiles batched tiles (any mix of P): as many
+// CTAs as the device holds at once, each taking tiles from the queue in
+// a.queue order by an atomic ticket (a.ticket must read 0 when the launch
+// starts).  The number of CTAs launched is returned in *ctas.
+cudaError_t launch_march_sum_queue(const SumArgs& a, int n_tiles, int form, cudaStream_t st, int* ctas);
+
 cudaError_t launch_march_sum(const SumArgs& a, const int* tile_P, int n_tiles, int form,
                              const cudaStream_t* streams, int n_streams, int* launches);
 

@@ -130,6 +130,26 @@ class Engine:
             pass
 
 
+def plan_columns(batch: Batch, row_step_s, updates_per_s):
+    """The column policy's cost rule for given costs (cr_plan_columns, host only):
+    a bool array, True for the rays whose lockstep march in a batched tile
+    would outlast the whole batch's balanced time by the policy's margin."""
+    lib = _lib.load()
+    rays = np.ascontiguousarray(batch.rays)
+    envs = np.ascontiguousarray(batch.envs)
+    pool = np.ascontiguousarray(batch.pool, dtype=np.float64)
+    desc = _lib.CrBatch()
+    desc.n_rays, desc.n_envs = len(rays), len(envs)
+    desc.rays, desc.envs, desc.pool = rays.ctypes.data, envs.ctypes.data, pool.ctypes.data
+    desc.pool_len = pool.size
+    desc.precision = _lib.CR_PLAIN_C128
+    desc.compute_grids = 1 if batch.compute_grids else 0
+    desc.line_len, desc.grid_len = batch.line_len, batch.grid_len
+    out = np.zeros(len(rays), np.int32)
+    _lib.check(lib.cr_plan_columns(ctypes.byref(desc), float(row_step_s), float(updates_per_s), out.ctypes.data))
+    return out.astype(bool)
+
+
 def march_static(batch: Batch, dev_out, stream=0):
     """Run ``cr_march_static``: a whole march that allocates nothing.
 

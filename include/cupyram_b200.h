@@ -26,7 +26,7 @@
 extern "C" {
 #endif
 
-#define CR_ABI_VERSION 2
+#define CR_ABI_VERSION 3
 /* Largest number of Pade terms a ray may use. */
 #define CR_MAX_NP 10
 
@@ -131,6 +131,15 @@ typedef struct cr_stats {
     int64_t device_bytes;     /* device memory held by the engine               */
     int32_t column_rays;      /* rays marched by the column-parallel kernel      */
     int32_t column_launches;  /* cluster launches of the last cr_march           */
+    int32_t queue_ctas;       /* CTAs of the persistent batched launch (0: none,
+                                 or one launch per lanes-per-ray value)        */
+    int32_t reserved;
+    double create_ms;         /* host wall time of cr_create                    */
+    double pade_ms;           /* host wall time of the device Pade sets in it   */
+    double tuner_row_step_s;  /* measured batched cost the column policy used:
+                                 one row of one step of a tile alone (0: the
+                                 policy was forced by CUPYRAM_B200_COL)         */
+    double tuner_updates_per_s; /* measured batched throughput it used          */
 } cr_stats;
 
 typedef struct cr_engine cr_engine;
@@ -219,6 +228,19 @@ int cr_last_error(const cr_engine* e, char* buf, size_t len);
 int cr_global_error(char* buf, size_t len);
 
 void cr_destroy(cr_engine* e);
+
+/*
+ * The cost rule the engine's column policy applies at cr_create, on the host:
+ * is_column[i] = 1 when ray i's lockstep march in a batched tile,
+ * (nz + 2)(nr + 4 + 4 x operator changes) x row_step_s, exceeds 1.25 x the
+ * whole batch's balanced time, sum(nz nr) / updates_per_s.  cr_create takes
+ * both costs from the engine's tuner (measured once per device and precision
+ * form; cr_stats.tuner_*), and sends a chosen ray to the column kernel when
+ * its column also fits a cluster.  No counterpart in the reference, which
+ * sizes one grid for all rays (cupyram/cupyram.py:596-597).
+ */
+int cr_plan_columns(const cr_batch* batch, double row_step_s, double updates_per_s,
+                    int32_t* is_column);
 
 /*
  * Engines take their device memory from a stream-ordered pool per device that

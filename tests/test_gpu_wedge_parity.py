@@ -91,3 +91,34 @@ def test_wedge_rays_chosen_vs_oracle(cuda_device, monkeypatch, wedge_sample, sch
         out = eng.run()
     d = np.concatenate([np.abs(tl - tr)[tr < 100.0] for _, tl, tr in _lines(b, out, ref)])
     assert np.sqrt(np.mean(d * d)) <= RMS_CHOSEN and d.max() <= MAX_CHOSEN, (np.sqrt(np.mean(d * d)), d.max())
+
+
+def test_work_queue_matches_per_order_launches(cuda_device, monkeypatch, wedge_sample):
+    """The persistent launch that takes tiles from the device work queue (any mix
+    of lanes per ray; np 4..8 gives 2..4 lanes) gives bit-identical lines to one
+    launch per lanes-per-ray value: the same tile code, only the order in which
+    CTAs take the tiles differs."""
+    b, ref = wedge_sample
+    monkeypatch.setenv("CUPYRAM_B200_COL", "0")
+    outs = {}
+    for q in ("1", "0"):
+        monkeypatch.setenv("CUPYRAM_B200_QUEUE", q)
+        with Engine(b) as eng:
+            outs[q] = eng.run()
+            st = eng.stats()
+        assert (st["queue_ctas"] > 0) == (q == "1")
+        assert st["kernel_launches"] == (1 if q == "1" else len(np.unique((b.rays["np"] + 1) // 2)))
+    assert np.array_equal(outs["1"]["tll"][:b.line_len], outs["0"]["tll"][:b.line_len])
+    assert np.array_equal(outs["1"]["cpl"][:b.line_len], outs["0"]["cpl"][:b.line_len])
+
+
+def test_tuner_costs_are_measured(cuda_device, monkeypatch, wedge_sample):
+    """The default policy reports the batched costs the engine's tuner measured on
+    this device (cr_stats.tuner_*), and they are of a plausible size."""
+    b, _ = wedge_sample
+    monkeypatch.delenv("CUPYRAM_B200_COL", raising=False)
+    monkeypatch.delenv("CUPYRAM_B200_COSTS", raising=False)
+    with Engine(b) as eng:
+        st = eng.stats()
+    assert 1e-8 < st["tuner_row_step_s"] < 1e-4
+    assert 1e8 < st["tuner_updates_per_s"] < 1e12
