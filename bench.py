@@ -62,7 +62,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "PE grid-point updates/s (1 B200) plain vs chosen form at ≤0.1 dB TL RMS error"
 UNIT = "grid-point updates/s"
-B_ALG = {"plain": 72.0, "chosen": 52.0, "fast": 52.0}  # algorithmic bytes per grid-point update
+B_ALG = {"plain": 72.0, "chosen": 52.0, "fast": 52.0, "refined": 52.0}  # algorithmic bytes per grid-point update
 
 
 def parse():
@@ -71,7 +71,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--form", choices=["plain", "chosen", "fast"], default="plain")
+    ap.add_argument("--form", choices=["plain", "chosen", "fast", "refined"], default="plain")
     ap.add_argument("--config", choices=["munk", "pekeris", "wedge", "precision", "surrogate", "gemm", "peaks"],
                     default="munk")
     ap.add_argument("--train", type=int, default=200_000, help="surrogate: training marches")
@@ -277,7 +277,9 @@ def tl_errors(tl_ref, tl):
 
 FORM_DESC = {"chosen": "complex64 factors and workspace, FP32 sweeps, FP64 term combination and field",
              "fast": "complex64 factors and workspace, FP32 inner loop (sweeps, couplings, M u and term "
-                     "combination in FP32); FP64 factorisation and field"}
+                     "combination in FP32); FP64 factorisation and field",
+             "refined": "the chosen form plus one iterative-refinement step per Pade term and range step: "
+                        "FP64 residual, correction solved with the same complex64 factors (two passes a step)"}
 
 
 def chosen_form(a, batch, out_plain, torch, world, pg, barrier, peak, form="chosen"):
@@ -535,7 +537,7 @@ def main():
     peak, peak_kind = measured_peak_hbm()
     reduced = {}  # form -> (bench record, TL line)
     if a.form == "plain" and not a.no_chosen:  # every rank takes part (max-over-ranks timing)
-        for form in ("chosen", "fast"):
+        for form in ("chosen", "fast", "refined"):
             reduced[form] = chosen_form(a, batch, out, torch, world, pg, barrier, peak, form)
     if rank != 0:
         if pg is not None:

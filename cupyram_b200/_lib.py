@@ -19,7 +19,7 @@ MAX_NP = 10
 # status codes (enum cr_status)
 CR_OK, CR_EINVAL, CR_ECUDA, CR_EPADE, CR_ETIMEOUT, CR_ENAN, CR_ENOMEM, CR_ESTATE = range(8)
 # precision forms (enum cr_precision)
-CR_PLAIN_C128, CR_CHOSEN_C64R, CR_CHOSEN_C64 = 0, 1, 2
+CR_PLAIN_C128, CR_CHOSEN_C64R, CR_CHOSEN_C64, CR_C64_REFINED = 0, 1, 2, 3
 
 RAY_DTYPE = np.dtype(
     [("freq", "f8"), ("c0", "f8"), ("zs", "f8"), ("zr", "f8"), ("dz", "f8"), ("dr", "f8"),
@@ -54,7 +54,7 @@ class CrStats(ctypes.Structure):
                 ("rays_failed", ctypes.c_int32), ("tile_rays", ctypes.c_int32),
                 ("n_tiles", ctypes.c_int32), ("device_bytes", ctypes.c_int64),
                 ("column_rays", ctypes.c_int32), ("column_launches", ctypes.c_int32),
-                ("queue_ctas", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("queue_ctas", ctypes.c_int32), ("precision_used", ctypes.c_int32),
                 ("create_ms", ctypes.c_double), ("pade_ms", ctypes.c_double),
                 ("tuner_row_step_s", ctypes.c_double), ("tuner_updates_per_s", ctypes.c_double)]
 

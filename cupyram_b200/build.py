@@ -1,20 +1,20 @@
 """Build the native engine in-tree: ``python -m cupyram_b200.build``.
 
-Compiles every ``csrc/*.cu`` for sm_100a (B200) into ``libcupyram_b200.so``
-next to this file.  nvcc cross-compiles, so no GPU is needed to build.
+Compiles every ``csrc/*.cu`` for sm_100a (B200), one process per file, and
+links ``libcupyram_b200.so`` next to this file.  nvcc cross-compiles, so no GPU is needed to build.
 """
 import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 OUT = HERE / "libcupyram_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-         "--expt-relaxed-constexpr"]
+CFLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 
 
 def nvcc():
@@ -36,14 +36,30 @@ def up_to_date():
     return all(d.stat().st_mtime <= t for d in deps if d.exists())
 
 
-def build(force=False, verbose=False):
-    if not force and up_to_date():
-        return OUT
-    cmd = [nvcc(), *ARCH, *FLAGS, "-I", str(HERE.parent / "include"), "-o", str(OUT) + ".tmp",
-           *map(str, sources())]
+def _compile(src, obj, verbose):
+    cmd = [nvcc(), *ARCH, *CFLAGS, "-I", str(HERE.parent / "include"), "-c", str(src), "-o", str(obj)]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    return obj
+
+
+def build(force=False, verbose=False, jobs=None):
+    """Compile every csrc/*.cu to an object in _build/ (in parallel: the three
+    precision forms of the batched march are separate translation units), then
+    link the shared library."""
+    if not force and up_to_date():
+        return OUT
+    objdir = HERE.parent / "_build"
+    objdir.mkdir(exist_ok=True)
+    srcs = sources()
+    objs = [objdir / (s.stem + ".o") for s in srcs]
+    n = jobs or min(len(srcs), os.cpu_count() or 1)
+    with ThreadPoolExecutor(max_workers=max(1, n)) as ex:
+        for f in [ex.submit(_compile, s, o, verbose) for s, o in zip(srcs, objs)]:
+            f.result()
+    cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", str(OUT) + ".tmp", *map(str, objs)]
     subprocess.run(cmd, check=True)
     os.replace(str(OUT) + ".tmp", OUT)
     return OUT

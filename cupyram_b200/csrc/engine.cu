@@ -621,6 +621,7 @@ struct cr_engine {
     long long* d_tile_loff = nullptr;
     double2 *d_pfc = nullptr, *d_pfcinf = nullptr;
     double2 *d_QD = nullptr, *d_WD = nullptr, *d_QU = nullptr, *d_WU = nullptr, *d_ED = nullptr, *d_EU = nullptr;
+    double2* d_E2 = nullptr;  // refined form: the rows' d2
     // column-parallel march: rays marched by one thread-block cluster each,
     // one launch per (Pade term count) group on its own stream
     struct ColGroup {
@@ -707,7 +708,7 @@ void free_all(cr_engine* e) {
                     e->d_tll,  e->d_cpl,  e->d_tlg,  e->d_cpg,      e->d_flags, e->d_S1, e->d_S2,
                     e->d_S3,   e->d_AL,   e->d_WF,   e->d_tile_G,  e->d_tile_off, e->d_tile_loff, e->d_pfc, e->d_pfcinf,
                     e->d_QD,   e->d_WD,   e->d_QU,   e->d_WU,      e->d_ED,  e->d_EU, e->d_col_ray,
-                    e->d_queue, e->d_ticket};
+                    e->d_queue, e->d_ticket, e->d_E2};
     // stream-ordered frees on the engine's stream (every other stream of the
     // engine joins it at the end of each march), back into the pool
     if (e->stream) {
@@ -794,8 +795,7 @@ std::string validate(const cr_batch* b) {
     if (b->n_rays < 1) return "n_rays must be >= 1";
     if (b->n_envs < 1) return "n_envs must be >= 1";
     if (!b->rays || !b->envs || !b->pool) return "rays, envs and pool must be non-NULL";
-    if (b->precision != CR_PLAIN_C128 && b->precision != CR_CHOSEN_C64R && b->precision != CR_CHOSEN_C64)
-        return "unknown precision form";
+    if (b->precision < CR_PLAIN_C128 || b->precision > CR_C64_REFINED) return "unknown precision form";
     for (int k = 0; k < b->n_envs; ++k) {
         const cr_env& v = b->envs[k];
         if (v.n_zss < 1 || v.n_rss < 1 || v.n_zsb < 1 || v.n_rsb < 1 || v.n_bt < 1) {
@@ -870,7 +870,11 @@ cudaError_t device_pade(const std::vector<PadeJob>& jobs, std::vector<double2>& 
     cudaStream_t st = nullptr;
     cudaError_t ce = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
     if (ce != cudaSuccess) return ce;
-    const size_t bj = jobs.size() * sizeof(PadeJob), bp = pd1.size() * sizeof(double2), bs = (size_t)n * sizeof(int);
+    // regions rounded up to 256 bytes: the coefficient arrays are double2 and
+    // must start on a 16-byte boundary whatever the number of jobs
+    auto r256 = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    const size_t bj = r256(jobs.size() * sizeof(PadeJob)), bp = r256(pd1.size() * sizeof(double2)),
+                 bs = r256((size_t)n * sizeof(int));
     unsigned char* d = nullptr;
     ce = cudaMallocAsync((void**)&d, bj + 2 * bp + bs, st);
     if (ce == cudaSuccess) {
@@ -878,16 +882,17 @@ cudaError_t device_pade(const std::vector<PadeJob>& jobs, std::vector<double2>& 
         double2* d1 = (double2*)(d + bj);
         double2* d2 = (double2*)(d + bj + bp);
         int* ds = (int*)(d + bj + 2 * bp);
-        ce = cudaMemcpyAsync(dj, jobs.data(), bj, cudaMemcpyHostToDevice, st);
+        ce = cudaMemcpyAsync(dj, jobs.data(), jobs.size() * sizeof(PadeJob), cudaMemcpyHostToDevice, st);
         if (ce == cudaSuccess) {
             // 32 threads a block: the solves are long serial chains, so the
             // jobs are spread over as many SMs as possible
             pade_batch_kernel<<<(n + 31) / 32, 32, 0, st>>>(dj, n, d1, d2, ds);
             ce = cudaGetLastError();
         }
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(pd1.data(), d1, bp, cudaMemcpyDeviceToHost, st);
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(pd2.data(), d2, bp, cudaMemcpyDeviceToHost, st);
-        if (ce == cudaSuccess) ce = cudaMemcpyAsync(status.data(), ds, bs, cudaMemcpyDeviceToHost, st);
+        const size_t np2 = pd1.size() * sizeof(double2);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(pd1.data(), d1, np2, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(pd2.data(), d2, np2, cudaMemcpyDeviceToHost, st);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(status.data(), ds, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, st);
         const cudaError_t cf = cudaFreeAsync(d, st);
         if (ce == cudaSuccess) ce = cf;
     }
@@ -1223,7 +1228,8 @@ thread_local bool g_in_tuner = false;  // set while the tuner's own batches are 
 // ray that fits, unset / other: the cost rule.
 std::vector<char> pick_column_rays(const cr_batch* b, const std::vector<int>& pd_n, int precision, int device,
                                    MarchCosts* used) {
-    const bool chosen = precision != CR_PLAIN_C128;
+    // the column kernel has no refinement: refined rays on it run complex128
+    const bool chosen = precision == CR_CHOSEN_C64R || precision == CR_CHOSEN_C64;
     std::vector<char> col((size_t)b->n_rays, 0);
     const char* env = getenv("CUPYRAM_B200_COL");
     const int mode = (env && env[0] == '0') ? 0 : ((env && env[0] == '1') ? 1 : 2);
@@ -1291,12 +1297,11 @@ int cr_create(const cr_batch* b, cr_engine** out) {
             if ((int)std::floor(b->rays[i].zs / b->rays[i].dz) < 1) ok = false;
         e->sum_mode = ok;
     }
-    if (b->precision != CR_PLAIN_C128 && !e->sum_mode) {
-        set_global_error("cr_create: the chosen complex64 form needs every source below the first depth cell "
-                         "(zs >= dz) and the partial-fraction march (CUPYRAM_B200_SUM != 0)");
-        delete e;
-        return CR_EINVAL;
-    }
+    // The reduced forms exist for the partial-fraction march only.  A batch
+    // with a source in the first depth cell marches in the product form, in
+    // complex128, whatever form was asked for: a drop-in still runs it, more
+    // accurately than asked (cr_stats.precision_used says so).
+    e->st.precision_used = e->sum_mode ? b->precision : CR_PLAIN_C128;
     if (e->sum_mode) {
         // c_inf and residues c_k of every Pade set (FP64, host)
         e->pfc.assign((size_t)b->n_rays * kSets * CR_MAX_NP, make_double2(0.0, 0.0));
@@ -1397,7 +1402,7 @@ int cr_create(const cr_batch* b, cr_engine** out) {
         for (int rid : order)
             if (is_col[(size_t)rid]) cord.push_back(rid);
         auto terms_of = [&](int rid) { return col_terms(e->pd_n, rid); };
-        const bool chosen = b->precision != CR_PLAIN_C128;
+        const bool chosen = b->precision == CR_CHOSEN_C64R || b->precision == CR_CHOSEN_C64;
         const std::vector<int> csize = column_clusters(b, e->pd_n, is_col, chosen);
         std::stable_sort(cord.begin(), cord.end(), [&](int x, int y) {
             const int tx = terms_of(x), ty = terms_of(y);
@@ -1524,6 +1529,7 @@ int cr_create(const cr_batch* b, cr_engine** out) {
             if (ce == cudaSuccess) ce = dev_alloc(e, pp, (size_t)e->lane_elems);
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_ED, (size_t)e->col_elems);
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_EU, (size_t)e->col_elems);
+        if (ce == cudaSuccess && b->precision == CR_C64_REFINED) ce = dev_alloc(e, &e->d_E2, (size_t)e->col_elems);
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tile_loff, e->tile_loff.size());
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_tile_G, e->tile_G.size());
         if (ce == cudaSuccess) ce = dev_alloc(e, &e->d_queue, e->queue.size());
@@ -1699,6 +1705,7 @@ int cr_march(cr_engine* e) {
         sa.WU = e->d_WU;
         sa.ED = e->d_ED;
         sa.EU = e->d_EU;
+        sa.E2 = e->d_E2;
         sa.tll = e->d_tll;
         sa.cpl = e->d_cpl;
         sa.tlg = e->d_tlg;
@@ -1724,7 +1731,7 @@ int cr_march(cr_engine* e) {
         ca.cpg = e->d_cpg;
         ca.flags = e->d_flags;
         ca.compute_grids = e->compute_grids;
-        const int chosen = e->precision != CR_PLAIN_C128;
+        const int chosen = e->precision == CR_CHOSEN_C64R || e->precision == CR_CHOSEN_C64;
         ce = cudaEventRecord(e->ev[0], e->stream);
         int nl = 0;
         // column groups first, each on its own stream (they hold the longest

@@ -1,907 +1,28 @@
-// march_sum.cu - range march in partial-fraction ("sum") form.
-//
-// The split-step Pade operator of one range step is a rational function of
-// the Galerkin operator X = M^{-1} D (M: mass matrix, D: Galerkin stiffness +
-// wavenumber rows; cupyram/fused_kernel.py:20-69):
-//
-//     P(X) = prod_j (1 + pd1_j X) / (1 + pd2_j X)          (reference: product form)
-//          = c_inf + sum_j c_j / (1 + pd2_j X)             (here: partial fractions)
-//
-// so u_new = c_inf u + sum_j c_j x_j with (M + pd2_j D) x_j = M u: the np
-// tridiagonal solves of a step are independent.  Each lane carries kT = 2
-// terms (two independent recurrence chains per row); a ray uses
-// P = ceil(np / kT) lanes and a warp holds floor(32 / P) rays.
-//
-// Per range step each lane runs ONE pass over its column:
-//   * the back-substitution of the previous step's solves of its terms,
-//   * the combination u_new = c_inf u_old + sum_j c_j x_j for the row: each
-//     lane sums its terms, the ray's P lanes exchange their sums by shuffles
-//     and add them in a fixed order (FP64, identical in every lane),
-//   * the elimination of the next step's solves two rows behind, so that the
-//     exchange latency is off the elimination's path,
-// alternating the pass direction every step.  Every lane of a warp visits
-// the same row index at the same iteration (the warp's deepest ray sets the
-// count), so the warp runs in lockstep.  The Thomas factorisation of each
-// term (1/den, the coupling factor and w per row, both directions) is
-// computed once per change of the operator - profiles, bathymetry index or
-// Pade set - and streamed from HBM, with the workspace g, through a per-lane
-// cp.async prefetch ring.  Only 1/den and w are stored per term; the
-// elimination's coupling factor -(a1 + pd2 e) / den is rebuilt in FP64 from
-// 1/den and the row's Galerkin coupling e (d1 going down, d3 going up,
-// complex128), which is stored once per ray row and shared by the ray's
-// terms.  The solve loop
-// handles kU rows per iteration so that one row's term exchange overlaps the
-// next row's recurrences.
-//
-// The sum form is the reference's rational operator rearranged; on the
-// golden cases it matches the product form to <= 5e-8 dB (oracle mode "sum").
+// march_sum.cu - launchers of the batched partial-fraction march: dispatch on
+// the precision form to its translation unit (march_sum_plain.cu,
+// march_sum_chosen.cu, march_sum_fast.cu, march_sum_refined.cu; kernels in
+// march_sum_impl.cuh).
 #include <cuda_runtime.h>
 
-#include <algorithm>
-
-#include "march_common.cuh"
 #include "march_sum.cuh"
 
 namespace crk {
 
-namespace {
-
-constexpr int kSR = 8;                // prefetch depth (rows) per lane
-#ifndef CR_SUM_ROWS
-#define CR_SUM_ROWS 2
-#endif
-constexpr int kU = CR_SUM_ROWS;       // rows per solve-loop iteration
-constexpr int kFields = 2 + 3 * kT;   // u, e, then (W, G, Q) per term slot
-static_assert((kSR & (kSR - 1)) == 0, "kSR must be a power of two");
-static_assert(kSR % kU == 0, "the prefetch ring must hold whole iterations");
-
-struct SumSmem {
-    double2 q[kSR][kFields][kTile];
-};
-
-enum SumPass { kElimOnly = 0, kFusedP = 1, kBackOnly = 2, kFactor = 3 };
-
-// Arithmetic forms of the march (template parameter F):
-//   kPlain  (0): complex128 factors / workspace, FP64 recurrences;
-//   kChosen (1): complex64 factors / workspace, FP32 recurrences, the terms
-//                combined in FP64 and the history of the field in FP64;
-//   kFast   (2): complex64 factors / workspace and an FP32 inner loop: the
-//                elimination's coupling, M u, the term combination and the
-//                exchange of the ray's shares all in FP32, the couplings
-//                stored as complex64.
-// The factorisation itself and the stored field stay FP64 / complex128 in
-// every form.
-constexpr int kPlain = 0, kChosen = 1, kFast = 2;
-template <int F>
-struct Form;
-template <>
-struct Form<kPlain> {
-    using R = double;
-    using V = double2;  // factors / workspace / recurrences
-    using H = double2;  // field history and term combination
-    using E = double2;  // stored Galerkin coupling
-};
-template <>
-struct Form<kChosen> {
-    using R = float;
-    using V = float2;
-    using H = double2;
-    using E = double2;
-};
-template <>
-struct Form<kFast> {
-    using R = float;
-    using V = float2;
-    using H = float2;
-    using E = float2;
-};
-
-__device__ __forceinline__ double2 up2(double2 v) { return v; }
-__device__ __forceinline__ double2 up2(float2 v) { return make_double2((double)v.x, (double)v.y); }
-template <typename T>
-__device__ __forceinline__ T dn2(double2 v);
-template <>
-__device__ __forceinline__ double2 dn2<double2>(double2 v) { return v; }
-template <>
-__device__ __forceinline__ float2 dn2<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
-
-// Prec<R>: the stored precision of the factors / workspace.
-template <typename R>
-struct Prec;
-template <>
-struct Prec<double> {
-    using V = double2;
-    __device__ static __forceinline__ V mk(double2 v) { return v; }
-    __device__ static __forceinline__ double2 up(V v) { return v; }
-};
-template <>
-struct Prec<float> {
-    using V = float2;
-    __device__ static __forceinline__ V mk(double2 v) { return make_float2((float)v.x, (float)v.y); }
-    __device__ static __forceinline__ double2 up(V v) { return make_double2((double)v.x, (double)v.y); }
-};
-
-struct Lane {
-    int lane, k, gbase, P;  // k: lane index within the ray's P lanes
-    int rows;               // rows per lane column, common to the warp (its deepest ray's nz + 2)
-    int span;               // iterations per pass: rows rounded up to a multiple of kU
-    int nzmin;              // shallowest ray of the warp (bounds the unchecked iterations)
-    unsigned gmask;         // lanes of this ray
-    unsigned wmask;         // active lanes of the warp: every pass runs in lockstep over them
-    long long rcol;         // ray column base (f1..f3, ksq, u)
-    long long lcol;         // lane column base of term slot 0 (G and the factors)
-    long long lstride;      // elements between term slots of a lane column
-};
-
-struct Ops {
-    int nz;
-    double cfact, a1, a2;
-    double2 pole[kT];  // pd2 of this lane's terms in the active set
-    double2 ck[kT];    // partial-fraction residues (0 for slots without a term)
-    double2 cinf;      // c_inf of the ray for the active set
-    // FP32 copies for the fast form's inner loop
-    float a1f, a2f;
-    float2 polef[kT], ckf[kT], cinff;
-};
-
-template <typename R>
-__device__ __forceinline__ const typename Prec<R>::V* fac(const double2* p) {
-    return reinterpret_cast<const typename Prec<R>::V*>(p);
-}
-template <typename R>
-__device__ __forceinline__ typename Prec<R>::V* facw(double2* p) {
-    return reinterpret_cast<typename Prec<R>::V*>(p);
-}
-
-__device__ __forceinline__ float* sfl(SumSmem& S, int slot, int lane) { return (float*)&S.q[slot][0][lane]; }
-__device__ __forceinline__ float2* sks(SumSmem& S, int slot, int lane) { return (float2*)&S.q[slot][1][lane]; }
-
-// Stream row of iteration k: the same for every lane of the warp.
-template <bool DOWN>
-__device__ __forceinline__ int row_of(const Lane& L, int k) {
-    return DOWN ? k : L.span - 1 - k;
-}
-
-// Copies for stream row r of a factor pass (one commit group, empty outside
-// the lane's rows).
-template <bool DOWN>
-__device__ __forceinline__ void sum_issue(const SumArgs& a, const Lane& L, SumSmem& S, int slot, int r, int nz) {
-    if (r >= 0 && r <= nz + 1) {
-        const long long ro = L.rcol + (long long)r * kTile;
-        float* f = sfl(S, slot, L.lane);
-        cp4(f + 0, a.f1 + ro);
-        cp4(f + 1, a.f2 + ro);
-        cp4(f + 2, a.f3 + ro);
-        cp8(sks(S, slot, L.lane), a.ksq + ro);
-    }
-    cp_commit();
-}
-
-// Column pointers of one solve pass (element 0 of the lane's columns).
-template <int F>
-struct PassPtrs {
-    using V = typename Form<F>::V;
-    using E = typename Form<F>::E;
-    double2* u;        // field (ray column)
-    const E* e;        // Galerkin coupling of this pass's elimination (ray column)
-    const V* w[kT];    // w of the solves being back-substituted (eliminated the other way)
-    V* g[kT];          // workspace: read by the back-substitution, rewritten by the elimination
-    const V* q[kT];    // 1/den of this pass's elimination
-};
-
-template <int F, bool DOWN>
-__device__ __forceinline__ PassPtrs<F> pass_ptrs(const SumArgs& a, const Lane& L) {
-    using R = typename Form<F>::R;
-    using E = typename Form<F>::E;
-    PassPtrs<F> p;
-    p.u = a.u + L.rcol;
-    p.e = reinterpret_cast<const E*>(DOWN ? a.ED : a.EU) + L.rcol;
-#pragma unroll
-    for (int t = 0; t < kT; ++t) {
-        const long long lo = L.lcol + t * L.lstride;
-        p.w[t] = fac<R>(DOWN ? a.WU : a.WD) + lo;
-        p.g[t] = facw<R>(a.G) + lo;
-        p.q[t] = fac<R>(DOWN ? a.QD : a.QU) + lo;
-    }
-    return p;
-}
-
-template <typename T>
-__device__ __forceinline__ void cpt(void* dst, const void* src) {
-    if (sizeof(T) == 16) cp16(dst, src);
-    else cp8(dst, src);
-}
-template <typename T>
-__device__ __forceinline__ void cptz(void* dst, const void* src, bool on) {
-    if (sizeof(T) == 16) cp16z(dst, src, on);
-    else cp8z(dst, src, on);
-}
-
-// Copies for stream row r of a solve pass (one commit group).  The
-// elimination works two rows behind the stream (row m = r -/+ 2).  CHECK:
-// rows outside the lane's column are copied with zero source size (no
-// global read; the slot is zero-filled).  Without CHECK every row involved
-// is an interior row of every ray of the warp.
-template <int F, int PASS, bool DOWN, bool CHECK>
-__device__ __forceinline__ void solve_issue(const PassPtrs<F>& p, const Lane& L, SumSmem& S, int slot, int r,
-                                            int nz) {
-    using V = typename Form<F>::V;
-    using E = typename Form<F>::E;
-    const bool on = CHECK ? ((r >= 0) & (r <= nz + 1)) : true;
-    const int ro = (CHECK ? (on ? r : 0) : r) * kTile;
-    const bool uon = PASS == kElimOnly ? on : (on & (L.k == 0));
-    if (CHECK || PASS != kElimOnly) cp16z(&S.q[slot][0][L.lane], p.u + ro, uon);
-    else cp16(&S.q[slot][0][L.lane], p.u + ro);
-    const int m = DOWN ? r - 2 : r + 2;
-    const bool mon = CHECK ? (on & (m >= 1) & (m <= nz)) : true;
-    const int mo = (CHECK ? (mon ? m : 0) : m) * kTile;
-    if (PASS != kBackOnly) {
-        if (CHECK) cptz<E>(&S.q[slot][1][L.lane], p.e + mo, mon);
-        else cpt<E>(&S.q[slot][1][L.lane], p.e + mo);
-    }
-#pragma unroll
-    for (int t = 0; t < kT; ++t) {
-        if (PASS != kElimOnly) {
-            if (CHECK) {
-                cptz<V>(&S.q[slot][2 + 3 * t][L.lane], p.w[t] + ro, on);
-                cptz<V>(&S.q[slot][3 + 3 * t][L.lane], p.g[t] + ro, on);
-            } else {
-                cpt<V>(&S.q[slot][2 + 3 * t][L.lane], p.w[t] + ro);
-                cpt<V>(&S.q[slot][3 + 3 * t][L.lane], p.g[t] + ro);
-            }
-        }
-        if (PASS != kBackOnly) {
-            if (CHECK) cptz<V>(&S.q[slot][4 + 3 * t][L.lane], p.q[t] + mo, mon);
-            else cpt<V>(&S.q[slot][4 + 3 * t][L.lane], p.q[t] + mo);
-        }
-    }
-    cp_commit();
-}
-
-// Thomas factorisation of (M + pole_t D) for this lane's terms, one direction.
-// The arithmetic is FP64 in every form; 1/den and w are stored in the sweep
-// precision, the row's Galerkin coupling in the form's coupling precision.
-template <int F, bool DOWN>
-__device__ void sum_factor(const SumArgs& a, const Lane& L, SumSmem& S, const Ops& o) {
-    using R = typename Form<F>::R;
-    using E = typename Form<F>::E;
-    using P = Prec<R>;
-    const int nz = o.nz;
-    __threadfence_block();
-#pragma unroll 1
-    for (int k = 0; k < kSR; ++k) sum_issue<DOWN>(a, L, S, k, row_of<DOWN>(L, k), nz);
-    EnvRow em{}, ec{}, ep{};
-    double2 wp[kT];
-#pragma unroll
-    for (int t = 0; t < kT; ++t) wp[t] = c2(0.0, 0.0);
-    typename P::V* Q = facw<R>(DOWN ? a.QD : a.QU);
-    E* Ecol = reinterpret_cast<E*>(DOWN ? a.ED : a.EU);
-    typename P::V* W = facw<R>(DOWN ? a.WD : a.WU);
-    int seen = 0;  // rows of this lane already streamed
-#pragma unroll 1
-    for (int k = 0; k < L.span; ++k) {
-        const int r = row_of<DOWN>(L, k);  // rows outside 0..nz+1: idle iterations
-        const int slot = k & (kSR - 1);
-        cp_wait<kSR - 1>();
-        EnvRow er;
-        {
-            const float* f = sfl(S, slot, L.lane);
-            er.f1 = f[0];
-            er.f2 = f[1];
-            er.f3 = f[2];
-            er.k = *sks(S, slot, L.lane);
-        }
-        sum_issue<DOWN>(a, L, S, slot, row_of<DOWN>(L, k + kSR), nz);
-        if (r < 0 || r > nz + 1) continue;
-        if (DOWN) {
-            em = ec;
-            ec = ep;
-            ep = er;
-        } else {
-            ep = ec;
-            ec = em;
-            em = er;
-        }
-        if (++seen < 3) continue;
-        const int m = DOWN ? r - 1 : r + 1;
-        if (m < 1 || m > nz) continue;
-        const Drow d = galerkin3(em, ec, ep, o.cfact);
-        if (L.k == 0) Ecol[L.rcol + (long long)m * kTile] = dn2<E>(DOWN ? d.d1 : d.d3);
-#pragma unroll
-        for (int t = 0; t < kT; ++t) {
-            const double2 r1 = caxpd(o.a1, o.pole[t], d.d1), r2 = caxpd(o.a2, o.pole[t], d.d2),
-                          r3 = caxpd(o.a1, o.pole[t], d.d3);
-            const double2 cin = DOWN ? r1 : r3, cout = DOWN ? r3 : r1;
-            const double2 q = crcp(cfms(r2, cin, wp[t]));
-            wp[t] = cmul(cout, q);
-            const long long mo = L.lcol + t * L.lstride + (long long)m * kTile;
-            Q[mo] = P::mk(q);
-            W[mo] = P::mk(wp[t]);
-        }
-    }
-    cp_wait<0>();
-}
-
-// g_m = q (M u)_m + al g_{m-/+1} for every term slot of the lane, with the
-// coupling factor al = -(a1 + pole e) q rebuilt from the stored 1/den q and
-// the row's Galerkin coupling e (the factorisation's own arithmetic).
-// Plain and chosen form M u and the coupling in FP64; the fast form does the
-// whole row in FP32 as g = q ((M u) - (a1 + pole e) g_prev).
-template <int F>
-__device__ __forceinline__ void elim_row(const Ops& o, typename Form<F>::H h3, typename Form<F>::H h2,
-                                         typename Form<F>::H h1, typename Form<F>::E fe,
-                                         const typename Form<F>::V* fq, typename Form<F>::V* gp) {
-    using R = typename Form<F>::R;
-    if constexpr (F == kFast) {
-        const float mx = fmaf(o.a1f, h3.x + h1.x, o.a2f * h2.x), my = fmaf(o.a1f, h3.y + h1.y, o.a2f * h2.y);
-#pragma unroll
-        for (int t = 0; t < kT; ++t) {
-            // cin = a1 + pole e;  v = M u - cin g_prev;  g = q v
-            const float cx = o.a1f + fmaf(o.polef[t].x, fe.x, -o.polef[t].y * fe.y);
-            const float cy = fmaf(o.polef[t].x, fe.y, o.polef[t].y * fe.x);
-            const float vx = fmaf(-cx, gp[t].x, fmaf(cy, gp[t].y, mx));
-            const float vy = fmaf(-cx, gp[t].y, fmaf(-cy, gp[t].x, my));
-            float2 g;
-            g.x = fmaf(fq[t].x, vx, -fq[t].y * vy);
-            g.y = fmaf(fq[t].x, vy, fq[t].y * vx);
-            gp[t] = g;
-        }
-    } else {
-        const double2 mud = c2(fma(o.a1, h3.x + h1.x, o.a2 * h2.x), fma(o.a1, h3.y + h1.y, o.a2 * h2.y));
-        const R mx = (R)mud.x, my = (R)mud.y;
-#pragma unroll
-        for (int t = 0; t < kT; ++t) {
-            // a1 + pole e cancels strongly for some terms: formed in FP64 like the
-            // factorisation, only al is rounded to the sweep precision
-            const double2 cin = caxpd(o.a1, o.pole[t], fe);
-            const double2 ci = cmul(cin, Prec<R>::up(fq[t]));
-            const R ax = (R)(-ci.x), ay = (R)(-ci.y);
-            const R tx = fma(fq[t].x, mx, -fq[t].y * my), ty = fma(fq[t].x, my, fq[t].y * mx);
-            typename Prec<R>::V g;
-            g.x = fma(ax, gp[t].x, fma(-ay, gp[t].y, tx));
-            g.y = fma(ax, gp[t].y, fma(ay, gp[t].x, ty));
-            gp[t] = g;
-        }
-    }
-}
-
-// One streamed row of a solve pass, in registers.
-template <int F>
-struct RowF {
-    using V = typename Form<F>::V;
-    double2 u;
-    typename Form<F>::E e;
-    V w[kT], g[kT], q[kT];
-};
-
-template <int F>
-__device__ __forceinline__ void load_row(const SumSmem& S, int slot, int lane, RowF<F>& f) {
-    using V = typename Form<F>::V;
-    using E = typename Form<F>::E;
-    f.u = S.q[slot][0][lane];
-    f.e = *reinterpret_cast<const E*>(&S.q[slot][1][lane]);
-#pragma unroll
-    for (int t = 0; t < kT; ++t) {
-        f.w[t] = *reinterpret_cast<const V*>(&S.q[slot][2 + 3 * t][lane]);
-        f.g[t] = *reinterpret_cast<const V*>(&S.q[slot][3 + 3 * t][lane]);
-        f.q[t] = *reinterpret_cast<const V*>(&S.q[slot][4 + 3 * t][lane]);
-    }
-}
-
-// Carried state of a solve pass.
-template <int F>
-struct SolveState {
-    using V = typename Form<F>::V;
-    typename Form<F>::H h1, h2, h3;  // u_new of the last three rows (h1 newest)
-    V xp[kT];                        // back-substitution chains
-    V gp[kT];                        // elimination chains
-};
-
-template <typename H>
-__device__ __forceinline__ H hsel(bool c, H a, H b) {
-    H r;
-    r.x = c ? a.x : b.x;
-    r.y = c ? a.y : b.y;
-    return r;
-}
-
-// Stream row r of a solve pass.  The elimination of row m = r -/+ 2 uses
-// (h3, h2, h1) = (u_{m-/+1}, u_m, u_{m+/-1}) and comes first; then the
-// back-substitution x_r = g_r - w_r x_{r-/+1} of each term and this lane's
-// share c_inf u_old (lane 0) + sum_t c_t x_t (FP64; FP32 in the fast form),
-// and the exchange of the ray's P shares, added in lane order (identical in
-// every lane).
-// CHECK: rows outside a ray's column are handled with selects and predicated
-// stores (branch-free); without CHECK, r and m are interior rows of every
-// ray of the warp and r is no ray's first back-substitution row.
-template <int F, int P, int PASS, bool DOWN, bool CHECK>
-__device__ __forceinline__ void solve_row(const PassPtrs<F>& p, const Lane& L, const Ops& o, const RowF<F>& f,
-                                          int r, SolveState<F>& st) {
-    using R = typename Form<F>::R;
-    using V = typename Form<F>::V;
-    using H = typename Form<F>::H;
-    const int nz = o.nz;
-    const R zr = R(0);
-    H hzero;
-    hzero.x = 0;
-    hzero.y = 0;
-    const bool valid = CHECK ? ((r >= 0) & (r <= nz + 1)) : true;
-    const bool interior = CHECK ? ((r >= 1) & (r <= nz)) : true;
-    if (PASS != kBackOnly) {
-        const int m = DOWN ? r - 2 : r + 2;
-        const bool mvalid = CHECK ? (valid & (m >= 1) & (m <= nz)) : true;
-        V g[kT];
-#pragma unroll
-        for (int t = 0; t < kT; ++t) g[t] = st.gp[t];
-        elim_row<F>(o, st.h3, st.h2, st.h1, f.e, f.q, g);
-        const int mo = (CHECK ? (mvalid ? m : 0) : m) * kTile;
-#pragma unroll
-        for (int t = 0; t < kT; ++t) {
-            if (mvalid) p.g[t][mo] = g[t];
-            if (CHECK) {
-                st.gp[t].x = mvalid ? g[t].x : st.gp[t].x;
-                st.gp[t].y = mvalid ? g[t].y : st.gp[t].y;
-            } else {
-                st.gp[t] = g[t];
-            }
-        }
-    }
-    H un;
-    if (PASS == kElimOnly) {
-        un = interior ? dn2<H>(f.u) : hzero;
-    } else {
-        const bool first = CHECK ? (DOWN ? (r == 1) : (r == nz)) : false;
-        H v;
-        if constexpr (F == kFast) {
-            const float2 uf = dn2<float2>(f.u);  // zero-filled except in lane 0
-            v.x = fmaf(o.cinff.x, uf.x, -o.cinff.y * uf.y);
-            v.y = fmaf(o.cinff.x, uf.y, o.cinff.y * uf.x);
-        } else {
-            v = cmul(o.cinf, f.u);  // f.u is zero-filled except in lane 0
-        }
-#pragma unroll
-        for (int t = 0; t < kT; ++t) {
-            V x;
-            x.x = fma(-f.w[t].x, st.xp[t].x, fma(f.w[t].y, st.xp[t].y, f.g[t].x));
-            x.y = fma(-f.w[t].x, st.xp[t].y, fma(-f.w[t].y, st.xp[t].x, f.g[t].y));
-            if (CHECK) {
-                x.x = first ? f.g[t].x : x.x;
-                x.y = first ? f.g[t].y : x.y;
-                x.x = interior ? x.x : zr;
-                x.y = interior ? x.y : zr;
-            }
-            st.xp[t] = x;
-            if constexpr (F == kFast) {
-                v.x = fmaf(o.ckf[t].x, x.x, fmaf(-o.ckf[t].y, x.y, v.x));
-                v.y = fmaf(o.ckf[t].x, x.y, fmaf(o.ckf[t].y, x.x, v.y));
-            } else {
-                const double2 xd = Prec<R>::up(x);
-                v = c2(fma(o.ck[t].x, xd.x, fma(-o.ck[t].y, xd.y, v.x)),
-                       fma(o.ck[t].x, xd.y, fma(o.ck[t].y, xd.x, v.y)));
-            }
-        }
-        H sh[P];
-#pragma unroll
-        for (int j = 0; j < P; ++j) {
-            sh[j].x = __shfl_sync(L.wmask, v.x, L.gbase + j);
-            sh[j].y = __shfl_sync(L.wmask, v.y, L.gbase + j);
-        }
-        H tot = sh[0];
-#pragma unroll
-        for (int j = 1; j < P; ++j) {
-            tot.x += sh[j].x;
-            tot.y += sh[j].y;
-        }
-        un = interior ? tot : hzero;
-        if (interior & (L.k == 0)) p.u[(CHECK ? (interior ? r : 0) : r) * kTile] = up2(un);
-    }
-    if (CHECK) {
-        st.h3 = hsel(valid, st.h2, st.h3);
-        st.h2 = hsel(valid, st.h1, st.h2);
-        st.h1 = hsel(valid, un, st.h1);
-    } else {
-        st.h3 = st.h2;
-        st.h2 = st.h1;
-        st.h1 = un;
-    }
-}
-
-// Iterations [k0, k1) of a solve pass, kU rows each.
-template <int F, int P, int PASS, bool DOWN, bool CHECK>
-__device__ __forceinline__ void solve_iters(const PassPtrs<F>& p, const Lane& L, SumSmem& S, const Ops& o, int k0,
-                                            int k1, SolveState<F>& st) {
-#pragma unroll 1
-    for (int k = k0; k < k1; k += kU) {
-        cp_wait<kSR - kU>();
-        RowF<F> f[kU];
-#pragma unroll
-        for (int j = 0; j < kU; ++j) load_row<F>(S, (k + j) & (kSR - 1), L.lane, f[j]);
-#pragma unroll
-        for (int j = 0; j < kU; ++j)
-            solve_issue<F, PASS, DOWN, CHECK>(p, L, S, (k + j) & (kSR - 1), row_of<DOWN>(L, k + j + kSR), o.nz);
-#pragma unroll
-        for (int j = 0; j < kU; ++j) solve_row<F, P, PASS, DOWN, CHECK>(p, L, o, f[j], row_of<DOWN>(L, k + j), st);
-    }
-}
-
-// One solve pass.  kElimOnly: eliminate from the stored field u.  kFusedP:
-// back-substitute the pending solves, combine the terms into u_new (stored
-// by lane 0 of the ray), eliminate the next solves.  kBackOnly:
-// back-substitute and combine only.  Rows are streamed in the pass
-// direction, kU per iteration.
-template <int F, int P, int PASS, bool DOWN>
-__device__ void sum_pass(const SumArgs& a, const Lane& L, SumSmem& S, const Ops& o) {
-    using V = typename Form<F>::V;
-    using H = typename Form<F>::H;
-    const int nz = o.nz;
-    const PassPtrs<F> p = pass_ptrs<F, DOWN>(a, L);
-    __threadfence_block();
-    __syncwarp(L.wmask);
-#pragma unroll 1
-    for (int k = 0; k < kSR; ++k) solve_issue<F, PASS, DOWN, true>(p, L, S, k, row_of<DOWN>(L, k), nz);
-    SolveState<F> st;
-    st.h1.x = st.h1.y = 0;
-    st.h2 = st.h3 = st.h1;
-#pragma unroll
-    for (int t = 0; t < kT; ++t) {
-        st.xp[t].x = st.xp[t].y = 0;
-        st.gp[t].x = st.gp[t].y = 0;
-    }
-    // Iterations whose rows r (and elimination rows, and the rows they
-    // prefetch) are interior rows of every ray of the warp, and past every
-    // first back-substitution row, run unchecked:
-    //   DOWN: 3 <= r and r + kSR <= nzmin + 1;   UP: kSR <= r <= nzmin - 2.
-    const int lb = DOWN ? 3 : L.span + 1 - L.nzmin;
-    const int ub = DOWN ? L.nzmin + 2 - kSR - kU : L.span - kU - kSR;  // last steady start
-    const int k_lo = min(L.span, (max(lb, 0) + kU - 1) / kU * kU);
-    const int k_hi = ub < k_lo ? k_lo : min(L.span, (ub / kU) * kU + kU);
-    solve_iters<F, P, PASS, DOWN, true>(p, L, S, o, 0, k_lo, st);
-    solve_iters<F, P, PASS, DOWN, false>(p, L, S, o, k_lo, k_hi, st);
-    solve_iters<F, P, PASS, DOWN, true>(p, L, S, o, k_hi, L.span, st);
-    // The last row to eliminate (m = nz DOWN, m = 1 UP) would need stream row
-    // nz+2 / -1; its window (u_{m-1}, u_m, u_{m+1}) is already in the history.
-    if (PASS != kBackOnly) {
-        const int m = DOWN ? nz : 1;
-        V fq[kT];
-#pragma unroll
-        for (int t = 0; t < kT; ++t) fq[t] = p.q[t][m * kTile];
-        elim_row<F>(o, st.h3, st.h2, st.h1, p.e[m * kTile], fq, st.gp);
-#pragma unroll
-        for (int t = 0; t < kT; ++t) p.g[t][m * kTile] = st.gp[t];
-    }
-    (void)sizeof(H);
-    cp_wait<0>();
-    __threadfence_block();
-    __syncwarp(L.wmask);
-}
-
-// TL line / grid and CP line / grid of the field stored in the ray column.
-__device__ void sum_outputs(const SumArgs& a, const RayDev& ry, const Lane& L, int tlc, double r, int ir,
-                            double dir, int* flag) {
-    if (L.k != 0 || tlc < 0 || tlc >= ry.nvr) return;
-    auto urow = [&](int i) -> double2 {
-        if (i <= 0 || i > ry.nz) return c2(0.0, 0.0);
-        return a.u[L.rcol + (long long)i * kTile];
-    };
-    const double2 ua = urow(ir), ub = urow(ir + 1);
-    const double fa = a.f3[L.rcol + (long long)ir * kTile];
-    const double fb = a.f3[L.rcol + (long long)(ir + 1) * kTile];
-    const double2 cp = c2((1.0 - dir) * fa * ua.x + dir * fb * ub.x, (1.0 - dir) * fa * ua.y + dir * fb * ub.y);
-    const double amp = hypot(cp.x, cp.y);
-    if (!isfinite(amp)) *flag |= 1;
-    a.tll[ry.line_off + tlc] = tl_db(amp, r);
-    a.cpl[ry.line_off + tlc] = cp;
-    if (a.compute_grids && ry.grid_off >= 0) {
-        for (int j = 0; j < ry.nvz; ++j) {
-            const int row = (j + 1) * ry.ndz;
-            if (row > ry.nz + 1) break;
-            const double2 uj = urow(row);
-            const double fj = a.f3[L.rcol + (long long)row * kTile];
-            const double2 g = c2(uj.x * fj, uj.y * fj);
-            const long long o = ry.grid_off + (long long)j * ry.nvr + tlc;
-            a.tlg[o] = tl_db(hypot(g.x, g.y), r);
-            a.cpg[o] = g;
-        }
-    }
-}
-
-// Poles and residues of this lane's term slots (term j = k + t P) in a set.
-__device__ void set_ops(const SumArgs& a, int rid, int set, const Lane& L, Ops* o) {
-    const int n = a.pd_n[rid * kSets + set];
-    const long long base = ((long long)rid * kSets + set) * CR_MAX_NP;
-#pragma unroll
-    for (int t = 0; t < kT; ++t) {
-        const int j = L.k + t * L.P;
-        // slots without a term solve a copy of term 0 with weight 0
-        o->pole[t] = a.pd2[base + (j < n ? j : 0)];
-        o->ck[t] = j < n ? a.pfc[base + j] : c2(0.0, 0.0);
-        o->polef[t] = dn2<float2>(o->pole[t]);
-        o->ckf[t] = dn2<float2>(o->ck[t]);
-    }
-    o->cinf = a.pfcinf[(long long)rid * kSets + set];
-    o->cinff = dn2<float2>(o->cinf);
-}
-
-template <int F>
-__device__ void sum_refactor(const SumArgs& a, const Lane& L, SumSmem& S, const Ops& o) {
-    sum_factor<F, true>(a, L, S, o);
-    sum_factor<F, false>(a, L, S, o);
-    __threadfence_block();
-    __syncwarp(L.wmask);
-}
-
-}  // namespace
-
-// The whole march of tile t (self-starter, every range step, the outputs) by
-// the calling warp; lanes without a ray return at once.
-template <int F, int P>
-__device__ __forceinline__ void march_tile(const SumArgs& a, SumSmem& S, int t) {
-    Lane L;
-    L.lane = threadIdx.x;
-    L.P = P;
-    const int rid = a.tile_ray[t * kTile + L.lane];
-    L.wmask = __ballot_sync(0xffffffffu, rid >= 0);
-    if (rid < 0 || a.tile_G[t] != P) return;
-    L.k = L.lane % L.P;
-    L.gbase = L.lane - L.k;
-    L.gmask = (L.P >= 32 ? 0xffffffffu : ((1u << L.P) - 1u)) << L.gbase;
-    const RayDev ry = a.rays[rid];
-    L.rcol = ry.col;
-    L.lcol = a.tile_loff[t] + L.lane;
-    // the warp marches in lockstep: every pass covers the deepest ray's rows,
-    // the step loop the longest ray's steps
-    L.rows = (int)__reduce_max_sync(L.wmask, (unsigned)(ry.nz + 2));
-    L.span = (L.rows + kU - 1) / kU * kU;
-    L.nzmin = (int)__reduce_min_sync(L.wmask, (unsigned)ry.nz);
-    L.lstride = (long long)L.rows * kTile;
-    const int nr_max = (int)__reduce_max_sync(L.wmask, (unsigned)ry.nr);
-    const EnvPtrs e = env_ptrs(a.envs[ry.env], a.pool);
-    const int nz = ry.nz;
-    int flag = 0;
-    Ops o;
-    o.nz = nz;
-    o.cfact = 0.5 / (ry.dz * ry.dz);
-    o.a1 = ry.k0 * ry.k0 / 6.0;
-    o.a2 = 2.0 * ry.k0 * ry.k0 / 3.0;
-    o.a1f = (float)o.a1;
-    o.a2f = (float)o.a2;
-
-    // initial profiles, split over the ray's lanes (cupyram.py:571-608, profl)
-    int iz = max(1, min(nz - 1, (int)floor(e.zb[0] / ry.dz)));
-    int ss = 0, sb = 0, bt = 0;
-    for (int i = L.k; i <= nz + 1; i += L.P) {
-        assemble_rows(ry, e, ss, sb, iz, i, i, a.f1, a.f2, a.f3, a.ksq);
-        a.u[L.rcol + (long long)i * kTile] = c2(0.0, 0.0);
-    }
-    __threadfence_block();
-    __syncwarp(L.wmask);
-    // self-starter delta (cupyram.py:1008-1022)
-    if (L.k == 0) {
-        const double si = ry.zs / ry.dz;
-        const int is = (int)floor(si);
-        const double dis = si - is;
-        const double amp = sqrt(2.0 * M_PI / ry.k0);
-        const double step = ry.zmax / (double)(nz + 1);
-        for (int q = 0; q < 2; ++q) {
-            const int i = is + q;
-            const double z = (i == nz + 1) ? ry.zmax : (double)i * step;
-            const RowProps p = row_props(e, ss, sb, z, ry.lyrw_lambda, ry.attnf);
-            const double alpw = sqrt((double)p.cw / ry.c0);
-            const double wgt = (q == 0) ? (1.0 - dis) : dis;
-            if (i >= 1 && i <= nz) a.u[L.rcol + (long long)i * kTile] = c2(wgt * amp / (ry.dz * alpw), 0.0);
-        }
-    }
-    __threadfence_block();
-    __syncwarp(L.wmask);
-
-    const double ri = ry.zr / ry.dz;
-    const int ir = (int)floor(ri);
-    const double dir = ri - ir;
-    int mdr = 0, tlc = -1;
-
-    // The step whose back-substitution is pending (warp-uniform direction);
-    // pend_valid is per ray: false once a ray has emitted its last step.
-    bool pend_down = true;
-    bool pend_valid = false;
-    bool pend_out = false;
-    double pend_r = 0.0;
-
-    // the output of the pending step is written once its back-substitution
-    // has stored the field (pass-level bookkeeping, inlined by hand so that
-    // no local escapes into a call and the lane state stays in registers)
-#define CR_FINISH_PENDING()                                                 \
-    do {                                                                    \
-        if (pend_valid && pend_out && ++mdr == ry.ndr) {                    \
-            mdr = 0;                                                        \
-            ++tlc;                                                          \
-            sum_outputs(a, ry, L, tlc, pend_r, ir, dir, &flag);             \
-        }                                                                   \
-        pend_valid = false;                                                 \
-        __syncwarp(L.wmask);                                                \
-    } while (0)
-#define CR_BACK_ONLY()                                                      \
-    do {                                                                    \
-        if (pend_down) sum_pass<F, P, kBackOnly, false>(a, L, S, o);        \
-        else sum_pass<F, P, kBackOnly, true>(a, L, S, o);                   \
-        CR_FINISH_PENDING();                                                \
-    } while (0)
-
-    // self-starter: two steps of 1/(1-X), one of the ip=2 operator
-    set_ops(a, rid, 0, L, &o);
-    sum_refactor<F>(a, L, S, o);
-    sum_pass<F, P, kElimOnly, true>(a, L, S, o);
-    pend_down = true;
-    pend_valid = true;
-    pend_out = false;
-    sum_pass<F, P, kFusedP, false>(a, L, S, o);  // back-substitute step 1, eliminate step 2 (UP)
-    CR_FINISH_PENDING();
-    pend_down = false;
-    pend_valid = true;
-    CR_BACK_ONLY();
-    set_ops(a, rid, 1, L, &o);
-    sum_refactor<F>(a, L, S, o);
-    sum_pass<F, P, kElimOnly, true>(a, L, S, o);
-    pend_down = true;
-    pend_valid = true;
-    pend_out = true;
-    pend_r = ry.dr;  // first output at r = dr (cupyram.py:703)
-
-    int set = 2;
-    double rs = ry.rs;
-    double r = ry.dr;
-    bool first_march = true;
-    for (int rn = 0; rn < nr_max; ++rn) {
-        const bool live = rn < ry.nr;
-        // updat (updat.py:38-140) for the step about to be taken
-        bool reprofile = false;
-        int iz_new = iz;
-        int new_set = set;
-        bool change = false;
-        if (live) {
-            if (e.n_bt > 1) {
-                while (bt < e.n_bt - 1 && r >= e.rb[bt + 1]) ++bt;
-                const int b1 = min(bt + 1, e.n_bt - 1);
-                const double r0 = e.rb[bt], r1 = e.rb[b1], z0 = e.zb[bt], z1 = e.zb[b1];
-                const double zc = (b1 == bt) ? z0 : z0 + (r + 0.5 * ry.dr - r0) * (z1 - z0) / (r1 - r0);
-                iz_new = max(1, min(nz - 1, (int)floor(zc / ry.dz)));
-            }
-            if (e.n_rss > 1) {
-                const int o2 = ss;
-                while (ss < e.n_rss - 1 && r >= e.rp_ss[ss + 1]) ++ss;
-                reprofile |= (ss != o2);
-            }
-            if (e.n_rsb > 1) {
-                const int o2 = sb;
-                while (sb < e.n_rsb - 1 && r >= e.rp_sb[sb + 1]) ++sb;
-                reprofile |= (sb != o2);
-            }
-            if (r >= rs) {  // stability constraints off (cupyram.py:976-999)
-                new_set = 3;
-                rs = INFINITY;
-            }
-            change = first_march || reprofile || iz_new != iz || new_set != set;
-        }
-        const double r_out = (double)(rn + 2) * ry.dr;
-        if (__any_sync(L.wmask, change)) {
-            // some ray of the warp changes its operator: finish the pending
-            // step alone, rebuild where needed, start this step from u
-            CR_BACK_ONLY();
-            if (change) {
-                if (reprofile) {
-                    for (int i = L.k; i <= nz + 1; i += L.P) assemble_rows(ry, e, ss, sb, iz_new, i, i, a.f1, a.f2, a.f3, a.ksq);
-                } else if (iz_new != iz) {
-                    const int lo = min(iz, iz_new) + 1, hi = max(iz, iz_new);
-                    for (int i = lo + L.k; i <= hi; i += L.P) assemble_rows(ry, e, ss, sb, iz_new, i, i, a.f1, a.f2, a.f3, a.ksq);
-                }
-                __threadfence_block();
-                __syncwarp(L.gmask);
-                iz = iz_new;
-                set = new_set;
-                set_ops(a, rid, set, L, &o);
-                sum_factor<F, true>(a, L, S, o);
-                sum_factor<F, false>(a, L, S, o);
-                __threadfence_block();
-            }
-            __syncwarp(L.wmask);
-            sum_pass<F, P, kElimOnly, true>(a, L, S, o);
-            pend_down = true;
-            first_march = false;
-        } else {
-            // back-substitute the pending step and eliminate this one in one pass
-            if (pend_down) sum_pass<F, P, kFusedP, false>(a, L, S, o);
-            else sum_pass<F, P, kFusedP, true>(a, L, S, o);
-            CR_FINISH_PENDING();
-            pend_down = !pend_down;
-        }
-        pend_valid = live;
-        pend_out = live;
-        pend_r = r_out;
-        r = r_out;
-    }
-    CR_BACK_ONLY();
-    if (L.k == 0) a.flags[rid] = flag;
-}
-
-#undef CR_FINISH_PENDING
-#undef CR_BACK_ONLY
-
-// One tile per CTA (one launch per lanes-per-ray value P).
-template <int F, int P>
-__global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    SumSmem& S = *reinterpret_cast<SumSmem*>(smem_raw);
-    march_tile<F, P>(a, S, a.tile_begin + blockIdx.x);
-}
-
-template <int F, int P = 1>
-__device__ __forceinline__ void march_tile_p(const SumArgs& a, SumSmem& S, int t, int p) {
-    if constexpr (P <= kMaxP) {
-        if (p == P) march_tile<F, P>(a, S, t);
-        else march_tile_p<F, P + 1>(a, S, t, p);
-    }
-}
-
-// Persistent march over every batched tile of the engine: each CTA (one
-// warp) takes the next tile from the device work queue - an atomic ticket
-// over a.queue, the tiles in longest-march-first order - until the queue is
-// empty, whatever its lanes per ray.  Taking a ticket never waits.
-template <int F>
-__global__ void __launch_bounds__(kTile) march_sum_queue_kernel(SumArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    SumSmem& S = *reinterpret_cast<SumSmem*>(smem_raw);
-    for (;;) {
-        int k = 0;
-        if (threadIdx.x == 0) k = atomicAdd(a.ticket, 1);
-        k = __shfl_sync(0xffffffffu, k, 0);
-        if (k >= a.n_queue) break;
-        const int t = a.queue[k];
-        march_tile_p<F>(a, S, t, a.tile_G[t]);
-        __syncwarp();
-    }
-}
-
-template <int F, int P>
-static cudaError_t launch_one(const SumArgs& a, int count, cudaStream_t st) {
-    const size_t smem = sizeof(SumSmem);
-    cudaError_t ce = cudaFuncSetAttribute(march_sum_kernel<F, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (ce != cudaSuccess) return ce;
-    march_sum_kernel<F, P><<<count, kTile, smem, st>>>(a);
-    return cudaGetLastError();
-}
-
-template <int F, int P = 1>
-static cudaError_t launch_p(const SumArgs& a, int p, int count, cudaStream_t st) {
-    if constexpr (P > kMaxP) {
-        return cudaErrorInvalidValue;
-    } else {
-        if (p == P) return launch_one<F, P>(a, count, st);
-        return launch_p<F, P + 1>(a, p, count, st);
-    }
-}
-
-template <int F>
-static cudaError_t launch_queue_f(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas) {
-    const size_t smem = sizeof(SumSmem);
-    cudaError_t ce = cudaFuncSetAttribute(march_sum_queue_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem);
-    if (ce != cudaSuccess) return ce;
-    int dev = 0, sms = 0, per_sm = 0;
-    ce = cudaGetDevice(&dev);
-    if (ce == cudaSuccess) ce = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (ce == cudaSuccess)
-        ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, march_sum_queue_kernel<F>, kTile, smem);
-    if (ce != cudaSuccess) return ce;
-    // every resident slot of the device, and no more CTAs than tiles
-    *ctas = std::max(1, std::min(n_tiles, std::max(1, per_sm) * sms));
-    march_sum_queue_kernel<F><<<*ctas, kTile, smem, st>>>(a);
-    return cudaGetLastError();
-}
+cudaError_t sum_launch_plain(const SumArgs& a, int p, int count, cudaStream_t st);
+cudaError_t sum_launch_chosen(const SumArgs& a, int p, int count, cudaStream_t st);
+cudaError_t sum_launch_fast(const SumArgs& a, int p, int count, cudaStream_t st);
+cudaError_t sum_queue_plain(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas);
+cudaError_t sum_queue_chosen(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas);
+cudaError_t sum_queue_fast(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas);
+cudaError_t sum_launch_refined(const SumArgs& a, int p, int count, cudaStream_t st);
+cudaError_t sum_queue_refined(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas);
 
 cudaError_t launch_march_sum_queue(const SumArgs& a, int n_tiles, int form, cudaStream_t st, int* ctas) {
     if (n_tiles <= 0) return cudaSuccess;
-    return form == CR_CHOSEN_C64 ? launch_queue_f<kFast>(a, n_tiles, st, ctas)
-           : form == CR_CHOSEN_C64R ? launch_queue_f<kChosen>(a, n_tiles, st, ctas)
-                                    : launch_queue_f<kPlain>(a, n_tiles, st, ctas);
+    return form == CR_C64_REFINED ? sum_queue_refined(a, n_tiles, st, ctas)
+           : form == CR_CHOSEN_C64 ? sum_queue_fast(a, n_tiles, st, ctas)
+           : form == CR_CHOSEN_C64R ? sum_queue_chosen(a, n_tiles, st, ctas)
+                                    : sum_queue_plain(a, n_tiles, st, ctas);
 }
 
 cudaError_t launch_march_sum(const SumArgs& a0, const int* tile_P, int n_tiles, int form,
@@ -915,9 +36,10 @@ cudaError_t launch_march_sum(const SumArgs& a0, const int* tile_P, int n_tiles, 
         SumArgs a = a0;
         a.tile_begin = begin;
         const cudaStream_t st = streams[*launches % n_streams];
-        const cudaError_t ce = form == CR_CHOSEN_C64 ? launch_p<kFast>(a, tile_P[begin], end - begin, st)
-                               : form == CR_CHOSEN_C64R ? launch_p<kChosen>(a, tile_P[begin], end - begin, st)
-                                                        : launch_p<kPlain>(a, tile_P[begin], end - begin, st);
+        const cudaError_t ce = form == CR_C64_REFINED ? sum_launch_refined(a, tile_P[begin], end - begin, st)
+                               : form == CR_CHOSEN_C64 ? sum_launch_fast(a, tile_P[begin], end - begin, st)
+                               : form == CR_CHOSEN_C64R ? sum_launch_chosen(a, tile_P[begin], end - begin, st)
+                                                        : sum_launch_plain(a, tile_P[begin], end - begin, st);
         if (ce != cudaSuccess) return ce;
         ++*launches;
         begin = end;

@@ -35,6 +35,7 @@ struct SumArgs {
     double2* G;
     double2 *QD, *WD, *QU, *WU;  // lane columns: 1/den and w per term, both directions
     double2 *ED, *EU;            // ray columns: Galerkin coupling into the row (d1 down, d3 up)
+    double2* E2;                 // ray columns: the row's d2 (refined form only, else NULL)
     double* tll;
     double2* cpl;
     double* tlg;
@@ -53,7 +54,9 @@ struct SumArgs {
 // workspace and FP64 sweeps; CR_CHOSEN_C64R: complex64 factors / workspace
 // and FP32 sweeps (the buffers given for G and the factors are then read as
 // float2), terms combined in FP64; CR_CHOSEN_C64: as CR_CHOSEN_C64R with the
-// couplings (ED / EU read as float2), M u and the term combination in FP32.
+// couplings (ED / EU read as float2), M u and the term combination in FP32;
+// CR_C64_REFINED: as CR_CHOSEN_C64R with one FP64-residual refinement step per
+// term and range step (two passes per step; E2 holds the rows' d2).
 // Largest lanes-per-ray value the kernels are instantiated for (np <= 10).
 constexpr int kMaxP = (10 + kT - 1) / kT;
 // tile_P: host copy of tile_G.  One launch per run of equal P: run i goes

@@ -1,0 +1,15 @@
+// march_sum_chosen.cu - the batched partial-fraction march instantiated for one
+// precision form (kChosen; see march_sum_impl.cuh).
+#include "march_sum_impl.cuh"
+
+namespace crk {
+
+cudaError_t sum_launch_chosen(const SumArgs& a, int p, int count, cudaStream_t st) {
+    return launch_p<kChosen>(a, p, count, st);
+}
+
+cudaError_t sum_queue_chosen(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas) {
+    return launch_queue_f<kChosen>(a, n_tiles, st, ctas);
+}
+
+}  // namespace crk

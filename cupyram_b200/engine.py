@@ -9,8 +9,11 @@ from .batch import Batch
 
 # precision forms of the march (enum cr_precision): "plain" complex128;
 # "chosen" complex64 sweeps with the terms combined in FP64; "fast" complex64
-# sweeps with an FP32 inner loop (couplings, M u and the combination in FP32)
-PRECISIONS = {"plain": _lib.CR_PLAIN_C128, "chosen": _lib.CR_CHOSEN_C64R, "fast": _lib.CR_CHOSEN_C64}
+# sweeps with an FP32 inner loop (couplings, M u and the combination in FP32);
+# "refined" the chosen form plus one FP64-residual refinement step per term
+# and range step
+PRECISIONS = {"plain": _lib.CR_PLAIN_C128, "chosen": _lib.CR_CHOSEN_C64R, "fast": _lib.CR_CHOSEN_C64,
+              "refined": _lib.CR_C64_REFINED}
 
 
 class Engine:

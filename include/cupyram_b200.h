@@ -49,10 +49,16 @@ enum cr_precision {
     CR_CHOSEN_C64R = 1,  /* complex64 factors, workspace and sweeps (FP32 arithmetic);
                             the Pade terms are combined in FP64 and the field is
                             kept in complex128                                    */
-    CR_CHOSEN_C64 = 2    /* complex64 factors and workspace with an FP32 inner loop:
+    CR_CHOSEN_C64 = 2,   /* complex64 factors and workspace with an FP32 inner loop:
                             sweeps, couplings, M u and the term combination in
                             FP32; the factorisation and the stored field stay
                             FP64 / complex128                                     */
+    CR_C64_REFINED = 3   /* CR_CHOSEN_C64R plus one iterative-refinement step per
+                            Pade term and range step: the residual
+                            M u - (M + pd2 D) x of the complex64 solve in FP64,
+                            its correction solved with the same complex64
+                            factors and added.  Rays on the column kernel or
+                            in the product form run complex128 instead       */
 };
 
 /*
@@ -133,7 +139,10 @@ typedef struct cr_stats {
     int32_t column_launches;  /* cluster launches of the last cr_march           */
     int32_t queue_ctas;       /* CTAs of the persistent batched launch (0: none,
                                  or one launch per lanes-per-ray value)        */
-    int32_t reserved;
+    int32_t precision_used;   /* enum cr_precision the march runs in: the
+                                 batch's, except that a batch with a source in
+                                 the first depth cell (zs < dz) runs the
+                                 complex128 product form in every form         */
     double create_ms;         /* host wall time of cr_create                    */
     double pade_ms;           /* host wall time of the device Pade sets in it   */
     double tuner_row_step_s;  /* measured batched cost the column policy used:

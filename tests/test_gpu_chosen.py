@@ -24,7 +24,7 @@ def _errs(ref, tl):
     return d.max(), np.sqrt(np.mean(d * d))
 
 
-@pytest.mark.parametrize("form", ["chosen", "fast"])
+@pytest.mark.parametrize("form", ["chosen", "fast", "refined"])
 @pytest.mark.parametrize("march", ["batched", "column"])
 @pytest.mark.parametrize("name", CASES)
 def test_chosen_vs_plain_golden(cuda_device, monkeypatch, name, march, form):
@@ -44,7 +44,7 @@ def test_chosen_vs_plain_golden(cuda_device, monkeypatch, name, march, form):
     assert rms <= RMS_DB, (mx, rms)
 
 
-@pytest.mark.parametrize("form", ["chosen", "fast"])
+@pytest.mark.parametrize("form", ["chosen", "fast", "refined"])
 def test_chosen_vs_plain_munk_batch(cuda_device, form):
     b = workloads.build(*workloads.munk_batch(160, seed=11, rmax=20000.0), compute_grids=False)
     with Engine(b, precision="plain") as e1:
@@ -55,11 +55,35 @@ def test_chosen_vs_plain_munk_batch(cuda_device, form):
     assert rms <= RMS_DB and mx <= MAX_DB, (mx, rms)
 
 
-def test_chosen_rejected_for_surface_source(cuda_device):
+@pytest.mark.parametrize("form", ["chosen", "fast", "refined"])
+def test_reduced_forms_run_surface_sources(cuda_device, form):
+    """zs < dz puts the source in the surface row, where only the product-form march
+    applies; the reduced forms then run it in complex128 (reported in
+    cr_stats.precision_used) and match the oracle like the plain form."""
+    from oracle import oracle
+    from cupyram_b200 import _lib
     args, kw, _ = load_case("pekeris_small")
     args = list(args)
-    args[1] = 2.0  # zs < dz: product-form fallback, which has no chosen form
+    args[1] = 2.0  # zs = 2 m < dz = 3 m
     envs, p, zs, zr, pr = B.prepare(*args, dict(kw))
     b = B.build_batch(envs, p, zs, zr, pr, False)
-    with pytest.raises(ValueError, match="chosen"):
-        Engine(b, precision="chosen")
+    with Engine(b, precision=form) as eng:
+        out = eng.run()
+        assert eng.stats()["precision_used"] == _lib.CR_PLAIN_C128
+    ref = oracle.run(b, "plain")
+    assert np.abs(out["tll"][:b.line_len] - ref["tll"][:b.line_len]).max() < 1e-3
+
+
+def test_refinement_step_recovers_complex128(cuda_device, monkeypatch):
+    """The refined form's FP64-residual correction removes most of the complex64
+    solves' error: on the Munk rays its TL line is several times closer to the
+    complex128 march than the unrefined chosen form's, and within 0.01 dB."""
+    monkeypatch.setenv("CUPYRAM_B200_COL", "0")
+    b = workloads.build(*workloads.munk_batch(64, seed=13, rmax=20000.0), compute_grids=False)
+    outs = {}
+    for form in ("plain", "chosen", "refined"):
+        with Engine(b, precision=form) as eng:
+            outs[form] = eng.run()["tll"][:b.line_len]
+    _, rms_c = _errs(outs["plain"], outs["chosen"])
+    mx_r, rms_r = _errs(outs["plain"], outs["refined"])
+    assert rms_r < 0.3 * rms_c and mx_r < 0.01, (rms_r, rms_c, mx_r)
