@@ -46,18 +46,23 @@ def _compile(src, obj, verbose):
 
 
 def build(force=False, verbose=False, jobs=None):
-    """Compile every csrc/*.cu to an object in _build/ (in parallel: the three
+    """Compile every csrc/*.cu to an object in _build/ (in parallel: the four
     precision forms of the batched march are separate translation units), then
-    link the shared library."""
+    link the shared library.  Objects newer than their source and than every
+    header are reused."""
     if not force and up_to_date():
         return OUT
     objdir = HERE.parent / "_build"
     objdir.mkdir(exist_ok=True)
     srcs = sources()
     objs = [objdir / (s.stem + ".o") for s in srcs]
-    n = jobs or min(len(srcs), os.cpu_count() or 1)
+    headers = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list((HERE.parent / "include").glob("*.h"))
+    newest_header = max((h.stat().st_mtime for h in headers), default=0.0)
+    stale = [(s, o) for s, o in zip(srcs, objs)
+             if force or not o.exists() or o.stat().st_mtime < max(s.stat().st_mtime, newest_header)]
+    n = jobs or min(max(len(stale), 1), os.cpu_count() or 1)
     with ThreadPoolExecutor(max_workers=max(1, n)) as ex:
-        for f in [ex.submit(_compile, s, o, verbose) for s, o in zip(srcs, objs)]:
+        for f in [ex.submit(_compile, s, o, verbose) for s, o in stale]:
             f.result()
     cmd = [nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", "-o", str(OUT) + ".tmp", *map(str, objs)]
     subprocess.run(cmd, check=True)

@@ -19,10 +19,12 @@
 //
 // Plus the small kernels of a training step: column sums (bias gradients),
 // the masked mean-squared-error gradient, Adam, and BF16 conversion.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 
 #include "../../include/cupyram_b200_mlp.h"
 
@@ -360,6 +362,159 @@ __global__ void __launch_bounds__(kUThreads) gemm_tn_umma(const __nv_bfloat16* _
 
 constexpr size_t kUSmem = 2 * kUStage + 1024 + 64;
 
+// ---------------------------------------------------------------------------
+// The tcgen05 contraction with its operands brought in by the tensor memory
+// accelerator (TMA) and its roles split over warps.
+//
+// Same block (128 x 256, FP32 accumulator in 256 TMEM columns), same
+// SWIZZLE_128B K-major tiles and MMAs as gemm_tn_umma, but:
+//   * lane 0 of warp 0 issues one cp.async.bulk.tensor per operand tile
+//     (tensor maps over this GPU's memory, no multicast) that completes on
+//     the stage's "full" mbarrier with the byte count it expects;
+//   * lane 0 of warp 1 waits on "full", issues the four k16 MMAs of the
+//     stage and commits them to the stage's "empty" mbarrier, which the
+//     producer waits on before refilling the stage: no __syncthreads and no
+//     thread-issued copies in the main loop;
+//   * kTStages stages ring through shared memory;
+//   * after the last commit every warp reads its 32 accumulator rows and
+//     stores them as gemm_tn_umma does.
+// Every wait is bounded; one that gives up sets *err and the kernel finishes
+// without the result.
+// ---------------------------------------------------------------------------
+constexpr int kTStages = 2;  // 2 x 48 KB: two CTAs share an SM (and its 512 TMEM columns)
+constexpr size_t kTSmem = (size_t)kTStages * kUStage + 1024 + 256;
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(kUThreads) gemm_tn_tma(const __grid_constant__ CUtensorMap mapA,
+                                                        const __grid_constant__ CUtensorMap mapB, int K, EpiArgs e,
+                                                        int* err) {
+    extern __shared__ __align__(1024) unsigned char usmem[];
+    unsigned char* base = (unsigned char*)(((uintptr_t)usmem + 1023) & ~(uintptr_t)1023);
+    auto tA = [&](int st) { return base + st * kUStage; };
+    auto tB = [&](int st) { return base + st * kUStage + kUTileA; };
+    uint64_t* full = (uint64_t*)(base + kTStages * kUStage);
+    uint64_t* empty = full + kTStages;
+    uint64_t* done = empty + kTStages;
+    uint32_t* taddr_s = (uint32_t*)(done + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int bm = blockIdx.y * UBM, bn = blockIdx.x * UBN;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(taddr_s)),
+                     "r"(UBN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 32) {
+        for (int s = 0; s < kTStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        mbar_init(done, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *taddr_s;
+    const int nk = K / UBK;
+    bool ok = true;
+
+    int issued = 0;  // producer: tiles whose loads were issued
+    if (warp == 0 && lane == 0) {
+        // producer: stage st is refilled once the MMAs that read it have completed
+        for (int kt = 0; kt < nk && ok; ++kt) {
+            const int st = kt % kTStages;
+            if (kt >= kTStages) ok &= mbar_wait(&empty[st], ((kt / kTStages) - 1) & 1);
+            if (!ok) break;
+            mbar_expect_tx(&full[st], (unsigned)kUStage);
+            tma_load_2d(tA(st), &mapA, kt * UBK, bm, &full[st]);
+            tma_load_2d(tB(st), &mapB, kt * UBK, bn, &full[st]);
+            issued = kt + 1;
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        for (int kt = 0; kt < nk && ok; ++kt) {
+            const int st = kt % kTStages;
+            ok &= mbar_wait(&full[st], (kt / kTStages) & 1);
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t sa = smem_u32(tA(st)), sb = smem_u32(tB(st));
+#pragma unroll
+            for (int k = 0; k < UBK / 16; ++k) {
+                const uint64_t da = umma_desc_sw128(sa + k * 32), db = umma_desc_sw128(sb + k * 32);
+                const uint32_t acc = (kt > 0 || k > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                    :
+                    : "r"(tmem), "l"(da), "l"(db), "r"(kUIdesc), "r"(acc)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&empty[st]))
+                         : "memory");
+        }
+        // the accumulator is complete once every MMA issued so far is
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_u32(done))
+                     : "memory");
+    }
+    __syncwarp();
+    // every thread: wait for the accumulator (bounded), then the epilogue
+    ok &= mbar_wait(done, 0);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // a role thread that gave up is seen by the whole CTA
+    ok = __syncthreads_and(ok ? 1 : 0) != 0;
+    if (!ok && warp == 0 && lane == 0) {
+        // no copy may still be writing this CTA's shared memory when it exits:
+        // wait (bounded) for the last load issued into each stage
+        for (int kt = issued - 1; kt >= 0 && kt >= issued - kTStages; --kt)
+            mbar_wait(&full[kt % kTStages], (kt / kTStages) & 1);
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(err, 1);
+    } else {
+        float* stg = reinterpret_cast<float*>(base) + warp * 32 * 33;  // the stage tiles are idle now
+#pragma unroll 1
+        for (int cc = 0; cc < UBN; cc += 32) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                uint32_t v[16];
+                const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(cc + 16 * h);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                    "[%16];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                      "=r"(v[15])
+                    : "r"(ta));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int j = 0; j < 16; ++j) stg[lane * 33 + 16 * h + j] = __uint_as_float(v[j]);
+            }
+            __syncwarp();
+#pragma unroll 4
+            for (int r = 0; r < 32; ++r) store1<EPI>(e, bm + warp * 32 + r, bn + cc + lane, stg[r * 33 + lane]);
+            __syncwarp();
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(UBN));
+}
+
 // dst[c][r] = src[r][c] for a rows x cols BF16 matrix (32 x 32 tiles).
 __global__ void transpose_bf16(const __nv_bfloat16* __restrict__ src, int lds, __nv_bfloat16* __restrict__ dst,
                                int ldd, int rows, int cols) {
@@ -438,6 +593,46 @@ int grid_for(long long n) {
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 
+// CUPYRAM_B200_GEMM=tma selects the TMA-fed kernel for cr_mlp_gemm_tc
+// (default: the cp.async-fed one).
+bool use_tma_gemm() {
+    const char* v = getenv("CUPYRAM_B200_GEMM");
+    return v && v[0] == 't';
+}
+
+// cuTensorMapEncodeTiled, reached through the runtime's driver entry point
+// (the library links no driver library).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+// Tensor map of a rows x K bf16 operand (row stride ld elements) in boxes of
+// `box_rows` rows x 64 elements, 128-byte swizzle: the layout the MMAs read.
+bool operand_map(CUtensorMap* map, const void* ptr, int rows, int K, int ld, int box_rows) {
+    EncodeTiledFn enc = encode_tiled();
+    if (!enc) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)UBK, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(ptr), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 }  // namespace
 
 extern "C" {
@@ -478,6 +673,26 @@ int cr_mlp_gemm_tc(int epi, const void* A, const void* B, int M, int N, int K, i
     auto a = (const __nv_bfloat16*)A;
     auto b = (const __nv_bfloat16*)B;
     cudaError_t ce = cudaSuccess;
+    if (use_tma_gemm()) {
+        // operands by the tensor memory accelerator (tensor maps over this GPU's memory)
+        CUtensorMap ma, mb;
+        if (!operand_map(&ma, A, M, K, lda, UBM) || !operand_map(&mb, B, N, K, ldb, UBN)) return CR_MLP_ECUDA;
+        switch (epi) {
+#define CR_TMA_CASE(E)                                                                                       \
+    case E:                                                                                                  \
+        ce = cudaFuncSetAttribute(gemm_tn_tma<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTSmem);   \
+        if (ce == cudaSuccess) gemm_tn_tma<E><<<grid, kUThreads, kTSmem, st>>>(ma, mb, K, e, err);            \
+        break;
+            CR_TMA_CASE(CR_MLP_EPI_BIAS_RELU_BF16)
+            CR_TMA_CASE(CR_MLP_EPI_BIAS_F32)
+            CR_TMA_CASE(CR_MLP_EPI_F32)
+            CR_TMA_CASE(CR_MLP_EPI_RELU_MASK_BF16)
+#undef CR_TMA_CASE
+            default: return CR_MLP_EBADSHAPE;
+        }
+        if (ce != cudaSuccess) return CR_MLP_ECUDA;
+        return cudaGetLastError() == cudaSuccess ? 0 : CR_MLP_ECUDA;
+    }
     switch (epi) {
 #define CR_UMMA_CASE(E)                                                                                    \
     case E:                                                                                                \

@@ -7,8 +7,8 @@ buffers the engine fills (tll, cpl and, with grids, tlg, cpg).
 Modes: ``"ref"`` (the reference's float32 / complex64 storage and workspace
 roundings), ``"plain"`` (the engine's plain complex128 form), ``"f64"``
 (everything FP64), ``"sum"`` (plain in partial-fraction form) and the
-chosen-form models ``"chosen"``, ``"chosen_c32"``, ``"chosen_f32"`` (see
-ram_oracle.c).  Parity of the oracle itself is pinned by
+chosen-form models ``"chosen"``, ``"chosen_c32"``, ``"chosen_f32"`` and the
+refined form's model ``"refined"`` (see ram_oracle.c).  Parity of the oracle itself is pinned by
 tests/test_oracle.py against tests/golden/ (the reference run on CPU under
 Numba's CUDA simulator) and RAM v1.5's published TL line.
 """
@@ -21,7 +21,8 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "libram_oracle.so"
-MODES = {"ref": 0, "plain": 1, "f64": 2, "sim": 3, "sum": 4, "chosen": 5, "chosen_c32": 6, "chosen_f32": 7}
+MODES = {"ref": 0, "plain": 1, "f64": 2, "sim": 3, "sum": 4, "chosen": 5, "chosen_c32": 6, "chosen_f32": 7,
+         "refined": 8}
 _lib = None
 
 

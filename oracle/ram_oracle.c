@@ -38,8 +38,13 @@
  *          FP64), M u rounded to complex64, the elimination and the
  *          back-substitution in FP32.  CHOSEN combines the terms in FP64
  *          (the engine's form); CHOSEN_C32 combines them in FP32; CHOSEN_F32
- *          also forms the coupling in FP32 from a complex64 d1.  Used by
- *          oracle/chosen_study.py to size the error of an FP32 inner loop.
+ *          also forms the coupling in FP32 from a complex64 d1 (the model of
+ *          the engine's fast form).
+ *   REFINED
+ *          the engine's refined form: CHOSEN, then per term one
+ *          iterative-refinement step - the residual of the complex64 solve
+ *          M u - (M + pd2 D) x against the FP64 Galerkin rows, its correction
+ *          solved with the same complex64 factors in FP32, added in FP64.
  *   SIM    REF plus the scalar promotions of Numba's CUDA simulator under
  *          NumPy 2 (a Python float times a float32 stays float32), which is
  *          how the golden fixtures were produced: the Galerkin c1..c3 are
@@ -67,6 +72,7 @@
 #define ORACLE_CHOSEN 5
 #define ORACLE_CHOSEN_C32 6
 #define ORACLE_CHOSEN_F32 7
+#define ORACLE_REFINED 8
 
 typedef double complex cd;
 
@@ -488,7 +494,8 @@ static inline cd to_c128(cf z) { return (double)crealf(z) + I * (double)cimagf(z
    downward elimination, complex64 factors and FP32 recurrences.  comb32:
    terms combined in FP32; coupling32: the coupling -(a1 + pd2 d1)/den
    formed in FP32 from a complex64 d1. */
-static void march_step_chosen(ray_state* s, int n, const cd* pd1, const cd* pd2, int comb32, int coupling32) {
+static void march_step_chosen(ray_state* s, int n, const cd* pd1, const cd* pd2, int comb32, int coupling32,
+                              int refine) {
     const int nz = s->nz;
     cd cinf = 1.0;
     for (int j = 0; j < n; ++j) cinf *= pd1[j] / pd2[j];
@@ -539,6 +546,30 @@ static void march_step_chosen(ray_state* s, int n, const cd* pd1, const cd* pd2,
         for (int i = 1; i <= nz; ++i) {
             acc[i] += ck * to_c128(x[i]);
             accf[i] += ckf * x[i];
+        }
+        if (refine) {
+            /* residual of the complex64 solve against the FP64 rows, and its
+               correction with the same complex64 factors */
+            cf* res = (cf*)malloc(sizeof(cf) * (size_t)(nz + 2));
+            for (int i = 1; i <= nz; ++i) {
+                galerkin(s, i, zero, pd2[k], r, rq);
+                const cd xm = i > 1 ? to_c128(x[i - 1]) : 0.0, xc = to_c128(x[i]),
+                         xp = i < nz ? to_c128(x[i + 1]) : 0.0;
+                const cd mud = a1 * (s->u[i - 1] + s->u[i + 1]) + a2 * s->u[i];
+                res[i] = to_c64(mud - (r[0] * xm + r[1] * xc + r[2] * xp));
+            }
+            cf gq = 0.0f;
+            for (int i = 1; i <= nz; ++i) {
+                gq = q[i] * res[i] + al[i] * gq;
+                g[i] = gq;
+            }
+            cf dx = g[nz];
+            acc[nz] += ck * to_c128(dx);
+            for (int i = nz - 1; i >= 1; --i) {
+                dx = g[i] - w[i] * dx;
+                acc[i] += ck * to_c128(dx);
+            }
+            free(res);
         }
     }
     for (int i = 1; i <= nz; ++i) s->u[i] = comb32 ? to_c128(accf[i]) : acc[i];
@@ -691,12 +722,14 @@ static int run_ray(const cr_batch* b, int ib, int mode, double* tll_all, double*
     for (int j = 0; j < CR_MAX_NP; ++j) { pd1[j] = 0.0; pd2[j] = 0.0; }
     pd2[0] = -1.0;
     const int nself = (mode == ORACLE_REF || mode == ORACLE_SIM) ? np : 1;
-    const int chosen = mode == ORACLE_CHOSEN || mode == ORACLE_CHOSEN_C32 || mode == ORACLE_CHOSEN_F32;
+    const int chosen = mode == ORACLE_CHOSEN || mode == ORACLE_CHOSEN_C32 || mode == ORACLE_CHOSEN_F32 ||
+                       mode == ORACLE_REFINED;
+    const int refine = mode == ORACLE_REFINED;
     const int comb32 = mode == ORACLE_CHOSEN_C32 || mode == ORACLE_CHOSEN_F32, coupling32 = mode == ORACLE_CHOSEN_F32;
     if (chosen) {
-        march_step_chosen(&s, 1, pd1, pd2, comb32, coupling32);
-        march_step_chosen(&s, 1, pd1, pd2, comb32, coupling32);
-        march_step_chosen(&s, np, sp1, sp2, comb32, coupling32);
+        march_step_chosen(&s, 1, pd1, pd2, comb32, coupling32, refine);
+        march_step_chosen(&s, 1, pd1, pd2, comb32, coupling32, refine);
+        march_step_chosen(&s, np, sp1, sp2, comb32, coupling32, refine);
     } else if (mode == ORACLE_SUM) {
         march_step_sum(&s, 1, pd1, pd2);
         march_step_sum(&s, 1, pd1, pd2);
@@ -720,7 +753,7 @@ static int run_ray(const cr_batch* b, int ib, int mode, double* tll_all, double*
             rs_lim = INFINITY;
         }
         init_profiles(&s);
-        if (chosen) march_step_chosen(&s, np, mp1, mp2, comb32, coupling32);
+        if (chosen) march_step_chosen(&s, np, mp1, mp2, comb32, coupling32, refine);
         else if (mode == ORACLE_SUM) march_step_sum(&s, np, mp1, mp2);
         else march_step(&s, np, mp1, mp2);
         r = (double)(rn + 2) * s.dr;

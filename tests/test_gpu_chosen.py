@@ -75,15 +75,21 @@ def test_reduced_forms_run_surface_sources(cuda_device, form):
 
 
 def test_refinement_step_recovers_complex128(cuda_device, monkeypatch):
-    """The refined form's FP64-residual correction removes most of the complex64
-    solves' error: on the Munk rays its TL line is several times closer to the
-    complex128 march than the unrefined chosen form's, and within 0.01 dB."""
+    """The refined form's FP64-residual correction removes the complex64 solves'
+    error: on Munk rays its TL line meets the plain form's parity bar against the
+    oracle's complex128 march (1e-3 dB), far closer than the unrefined chosen
+    form (the oracle's model of the refinement recovers FP64 to ~1e-10 dB)."""
+    from oracle import oracle
     monkeypatch.setenv("CUPYRAM_B200_COL", "0")
     b = workloads.build(*workloads.munk_batch(64, seed=13, rmax=20000.0), compute_grids=False)
     outs = {}
-    for form in ("plain", "chosen", "refined"):
+    for form in ("chosen", "refined"):
         with Engine(b, precision=form) as eng:
             outs[form] = eng.run()["tll"][:b.line_len]
-    _, rms_c = _errs(outs["plain"], outs["chosen"])
-    mx_r, rms_r = _errs(outs["plain"], outs["refined"])
-    assert rms_r < 0.3 * rms_c and mx_r < 0.01, (rms_r, rms_c, mx_r)
+    sample = [0, 21, 42, 63]
+    ref = oracle.run(b, "plain", rays=sample)["tll"]
+    for i in sample:
+        o, n = int(b.rays["line_off"][i]), int(b.rays["nvr"][i])
+        d_r = np.abs(outs["refined"][o:o + n] - ref[o:o + n])
+        d_c = np.abs(outs["chosen"][o:o + n] - ref[o:o + n])
+        assert d_r.max() < 1e-3 and d_r.max() < 0.1 * d_c.max(), (i, d_r.max(), d_c.max())

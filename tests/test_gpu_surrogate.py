@@ -42,12 +42,17 @@ def test_gemm_epilogues_vs_numpy(cuda_device):
         S.gemm(S.EPI_F32, _bf(A[:100]), Bb, out)  # M not a multiple of 128
 
 
-def test_gemm_tcgen05_vs_numpy(cuda_device):
-    """The tcgen05 kernel (accumulator in tensor memory) on every epilogue, and its wait flag clear."""
+@pytest.mark.parametrize("feed,M,N,K", [("cp.async", 256, 512, 192), ("tma", 256, 512, 192),
+                                         ("tma", 384, 768, 640)])
+def test_gemm_tcgen05_vs_numpy(cuda_device, monkeypatch, feed, M, N, K):
+    """The tcgen05 kernels (accumulator in tensor memory) on every epilogue, and their wait
+    flag clear: operands fed by per-thread cp.async, or by the tensor memory accelerator
+    with a producer warp and an MMA warp (CUPYRAM_B200_GEMM=tma; K of 192 and 640 run
+    the two-stage ring through 3 and 10 tiles)."""
     import torch
     from cupyram_b200 import surrogate as S
+    monkeypatch.setenv("CUPYRAM_B200_GEMM", "tma" if feed == "tma" else "")
     rng = np.random.default_rng(4)
-    M, N, K = 256, 512, 192
     A, B = rng.normal(size=(M, K)), rng.normal(size=(N, K))
     bias = rng.normal(size=N)
     mask = rng.normal(size=(M, N))

@@ -110,8 +110,8 @@ def test_oracle_batch_rays_independent():
 def test_chosen_form_models(name):
     """The oracle's chosen-form models (complex64 sweeps; FP64 or FP32 term
     combination; FP64 or FP32 coupling) round, and on these short cases stay
-    within 0.01 dB RMS of the FP64 sum form over cells with TL < 100 dB.
-    oracle/chosen_study.py runs them at the benchmark workloads' full ranges."""
+    within 0.01 dB RMS of the FP64 sum form over cells with TL < 100 dB
+    (the next test runs them at the Munk workload's full range)."""
     b, _ = _prep(name, False)
     ref = oracle.run(b, "sum")["tll"][: b.line_len]
     lit = ref < 100.0
@@ -124,7 +124,7 @@ def test_chosen_form_models_at_full_range():
     """Two full-range rays of the 4096-ray Munk batch (1999 steps, nz ~ 5600):
     the chosen-form model stays within 0.01 dB RMS of the FP64 sum form, and
     the all-FP32 inner loop within the chosen form's 0.1 dB RMS bar (cells with
-    TL < 100 dB); oracle/chosen_study.py gives the full table."""
+    TL < 100 dB)."""
     from cupyram_b200 import workloads
     b = workloads.build(*workloads.munk_batch(4096, seed=2024), compute_grids=False)
     rays = [0, 2048]
@@ -139,3 +139,18 @@ def test_chosen_form_models_at_full_range():
         for a, c in zip(ref, lines(mode)):
             d = (c - a)[a < 100.0]
             assert np.sqrt(np.mean(d * d)) < bar, (mode, np.sqrt(np.mean(d * d)))
+
+
+@pytest.mark.parametrize("name", ["mini_munk", "wedge_switch", "pekeris_small"])
+def test_refinement_model_recovers_fp64(name):
+    """The refined form's model: one FP64-residual correction per complex64 solve
+    brings the march back to the FP64 sum form (here to ~1e-10 dB), at least a
+    thousand times closer than the unrefined chosen model."""
+    b, _ = _prep(name, False)
+    ref = oracle.run(b, "sum")["tll"][: b.line_len]
+    lit = ref < 100.0
+    rms = {}
+    for mode in ("chosen", "refined"):
+        d = (oracle.run(b, mode)["tll"][: b.line_len] - ref)[lit]
+        rms[mode] = np.sqrt(np.mean(d * d))
+    assert rms["refined"] < 1e-3 * rms["chosen"] and rms["refined"] < 1e-8, rms
