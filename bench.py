@@ -563,7 +563,11 @@ def main():
                     "create_ms_per_step": float(np.mean(create_ms))},
             "e2e_resident": {"value": e2e_resident, "unit": UNIT,
                              "calls": "cr_run on an engine already created (upload, march, download)"},
-            "gpu_launches": int(launches), "clocks": clk.summary()}
+            "gpu_launches": int(launches), "clocks": clk.summary(),
+            "schedule": {"column_rays": int(st["column_rays"]), "column_launches": int(st["column_launches"]),
+                         "queue_ctas": int(st["queue_ctas"]), "tuner_row_step_s": st["tuner_row_step_s"],
+                         "tuner_updates_per_s": st["tuner_updates_per_s"],
+                         "create_ms": st["create_ms"], "pade_ms": st["pade_ms"]}}
     for form, (rec, _) in reduced.items():
         line[form] = rec
     if world == 1 and not a.no_cpu_baseline:

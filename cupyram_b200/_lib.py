@@ -64,7 +64,7 @@ _SIGS = {
     "cr_abi_version": (ctypes.c_int, []),
     "cr_pade": (ctypes.c_int, [ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int,
                                ctypes.c_double, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p]),
-    "cr_pade_batch": (ctypes.c_int, [ctypes.c_int] + [ctypes.c_void_p] * 10),
+    "cr_pade_batch": (ctypes.c_int, [ctypes.c_int] + [ctypes.c_void_p] * 9),
     "cr_create": (ctypes.c_int, [ctypes.POINTER(CrBatch), ctypes.POINTER(ctypes.c_void_p)]),
     "cr_upload": (ctypes.c_int, [ctypes.c_void_p]),
     "cr_march": (ctypes.c_int, [ctypes.c_void_p]),

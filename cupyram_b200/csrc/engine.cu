@@ -1757,6 +1757,11 @@ int cr_march(cr_engine* e) {
             int ctas = 0;
             if (ce == cudaSuccess && e->n_tiles > 0) ce = cudaMemsetAsync(e->d_ticket, 0, sizeof(int), e->stream);
             if (ce == cudaSuccess && e->n_tiles > 0) {
+                // beside column clusters, CTAs that stayed resident until the
+                // queue drained would hold SMs the clusters wait for: one CTA
+                // per tile then, taking the tiles in queue order and leaving
+                // as it finishes
+                sa.max_ctas = e->col_groups.empty() ? 0 : e->n_tiles;
                 ce = crk::launch_march_sum_queue(sa, e->n_tiles, e->precision, e->stream, &ctas);
                 nb = 1;
             }
@@ -1937,14 +1942,14 @@ int cr_plan_columns(const cr_batch* b, double row_step_s, double updates_per_s, 
 namespace {
 
 // The engine's own tuner: the two costs of the column policy, measured once
-// per device and precision form by marching synthetic batches through the
-// engine itself (all rays on the batched kernel):
-//   * one tile alone (10 rays of np 6, nz 2000, 30 steps): the time of one
-//     row of one step of a lockstep tile, the latency-bound case;
-//   * two rounds of tiles for every resident slot of the device (nz 200,
-//     40 steps): the batched kernel's throughput in grid-point updates/s.
-// About 0.1 s on first use; CUPYRAM_B200_COSTS="row_step_s,updates_per_s"
-// sets both instead (reproducible schedules).
+// per device and precision form by marching a synthetic batch through the
+// engine itself (every ray on the batched kernel): two rounds of tiles for
+// every resident slot of the device (10 rays of np 6 per tile, nz 200, 40
+// steps).  Its time gives the batched throughput in grid-point updates/s,
+// and - a round being one lockstep tile march per slot - the time of one row
+// of one step of a tile under that load.  About 0.1 s on first use;
+// CUPYRAM_B200_COSTS="row_step_s,updates_per_s" sets both instead
+// (reproducible schedules).
 std::mutex g_costs_mu;
 std::map<std::pair<int, int>, MarchCosts> g_costs;
 
@@ -1998,8 +2003,9 @@ void synth_batch(SynthBatch& s, int n_rays, int nz, int nr, int precision) {
     s.b.grid_len = 0;
 }
 
-// Device time (ms) of a warm march of a synthetic batch, or < 0 on failure.
-double synth_march_ms(int n_rays, int nz, int nr, int precision) {
+// Device time (ms) of a warm march of a synthetic batch, or < 0 on failure;
+// *ctas: the CTAs of its persistent batched launch.
+double synth_march_ms(int n_rays, int nz, int nr, int precision, int* ctas) {
     SynthBatch s;
     synth_batch(s, n_rays, nz, nr, precision);
     cr_engine* e = nullptr;
@@ -2007,7 +2013,10 @@ double synth_march_ms(int n_rays, int nz, int nr, int precision) {
     std::vector<double> tll((size_t)n_rays), cpl(2 * (size_t)n_rays);
     cr_outputs o{tll.data(), cpl.data(), nullptr, nullptr};
     double ms = -1.0;
-    if (cr_run(e, &o) == CR_OK && cr_march(e) == CR_OK) ms = e->st.march_ms;
+    if (cr_run(e, &o) == CR_OK && cr_march(e) == CR_OK) {
+        ms = e->st.march_ms;
+        *ctas = e->st.queue_ctas;
+    }
     cr_destroy(e);
     return ms;
 }
@@ -2027,15 +2036,16 @@ MarchCosts march_costs(int device, int precision) {
     c.updates_per_s = 1.3e10;
     g_in_tuner = true;
     {
-        const int nz1 = 2000, nr1 = 30;
-        const double t1 = synth_march_ms(10, nz1, nr1, precision);
-        int sms = 148;
+        int sms = 148, ctas = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        const int rays2 = 10 * 2 * 7 * sms, nz2 = 200, nr2 = 40;
-        const double t2 = synth_march_ms(rays2, nz2, nr2, precision);
-        // passes of a march without operator changes: about nr + 12 row sweeps
-        if (t1 > 0.0) c.row_step_s = t1 * 1e-3 / ((double)(nz1 + 2) * (double)(nr1 + 12));
-        if (t2 > 0.0) c.updates_per_s = (double)rays2 * nz2 * nr2 / (t2 * 1e-3);
+        const int nz = 200, nr = 40, rays = 10 * 2 * 7 * sms;
+        const double t = synth_march_ms(rays, nz, nr, precision, &ctas);
+        if (t > 0.0 && ctas > 0) {
+            const double tiles = (double)rays / 10.0;
+            c.updates_per_s = (double)rays * nz * nr / (t * 1e-3);
+            // a march without operator changes takes about nr + 12 row sweeps
+            c.row_step_s = t * 1e-3 * (double)ctas / tiles / ((double)(nz + 2) * (double)(nr + 12));
+        }
     }
     g_in_tuner = false;
     // the tuner's engines leave their memory in the pool: hand it back

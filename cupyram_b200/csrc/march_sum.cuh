@@ -48,6 +48,7 @@ struct SumArgs {
     int* ticket;
     const int* queue;
     int n_queue;
+    int max_ctas;  // persistent launch: CTAs = every resident slot (0), or this many
 };
 
 // form: an enum cr_precision value.  CR_PLAIN_C128: complex128 factors /

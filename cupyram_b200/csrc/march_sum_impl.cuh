@@ -1077,8 +1077,9 @@ static cudaError_t launch_queue_f(const SumArgs& a, int n_tiles, cudaStream_t st
     if (ce == cudaSuccess)
         ce = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, march_sum_queue_kernel<F>, kTile, smem);
     if (ce != cudaSuccess) return ce;
-    // every resident slot of the device, and no more CTAs than tiles
-    *ctas = std::max(1, std::min(n_tiles, std::max(1, per_sm) * sms));
+    // every resident slot of the device (or a.max_ctas), and no more CTAs than tiles
+    const int slots = a.max_ctas > 0 ? a.max_ctas : std::max(1, per_sm) * sms;
+    *ctas = std::max(1, std::min(n_tiles, slots));
     march_sum_queue_kernel<F><<<*ctas, kTile, smem, st>>>(a);
     return cudaGetLastError();
 }
