@@ -441,7 +441,9 @@ def run_gemm(a):
     flop = 2.0 * M * N * K
     peak, kind = measured_peak_bf16()
     res = {}
-    for name, tc in (("tcgen05", True), ("mma.sync", False)):
+    for name, tc, feed in (("tcgen05 (TMA-fed)", True, "tma"), ("tcgen05 (cp.async-fed)", True, "cp"),
+                           ("mma.sync", False, "cp")):
+        os.environ["CUPYRAM_B200_GEMM"] = feed
         for _ in range(a.warmup):
             S.gemm(S.EPI_BIAS_F32, A, B, out, bias=bias, tc=tc)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -454,10 +456,11 @@ def run_gemm(a):
         ms = e0.elapsed_time(e1) / a.steps
         res[name] = {"ms": ms, "tflops": flop / ms * 1e-9}
     assert int(S.tc_error_flag().item()) == 0
-    t = res["tcgen05"]["tflops"]
+    os.environ.pop("CUPYRAM_B200_GEMM", None)
+    t = res["tcgen05 (TMA-fed)"]["tflops"]
     line = {"metric": "surrogate GEMM TFLOP/s (bf16 x bf16 -> f32, 8192 x 8192 x 512)", "value": t,
             "unit": "TFLOP/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": res["tcgen05"]["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": res["tcgen05 (TMA-fed)"]["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "bf16", "data": "synthetic (random matrices)",
             "config": {"workload": "surrogate last-layer contraction, batch of 8192 requests", "config": "gemm",
                        "l2": "operands 16 MB (L2-resident); output 268 MB"},
@@ -566,7 +569,7 @@ def main():
             "gpu_launches": int(launches), "clocks": clk.summary(),
             "schedule": {"column_rays": int(st["column_rays"]), "column_launches": int(st["column_launches"]),
                          "queue_ctas": int(st["queue_ctas"]), "tuner_row_step_s": st["tuner_row_step_s"],
-                         "tuner_updates_per_s": st["tuner_updates_per_s"],
+                         "tuner_updates_per_s": st["tuner_updates_per_s"], "tuner_slots": st["tuner_slots"],
                          "create_ms": st["create_ms"], "pade_ms": st["pade_ms"]}}
     for form, (rec, _) in reduced.items():
         line[form] = rec

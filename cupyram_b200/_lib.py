@@ -56,7 +56,8 @@ class CrStats(ctypes.Structure):
                 ("column_rays", ctypes.c_int32), ("column_launches", ctypes.c_int32),
                 ("queue_ctas", ctypes.c_int32), ("precision_used", ctypes.c_int32),
                 ("create_ms", ctypes.c_double), ("pade_ms", ctypes.c_double),
-                ("tuner_row_step_s", ctypes.c_double), ("tuner_updates_per_s", ctypes.c_double)]
+                ("tuner_row_step_s", ctypes.c_double), ("tuner_updates_per_s", ctypes.c_double),
+                ("tuner_slots", ctypes.c_double)]
 
 
 # every symbol the header declares, with its signature
@@ -81,7 +82,7 @@ _SIGS = {
     "cr_destroy": (None, [ctypes.c_void_p]),
     "cr_release_cache": (ctypes.c_int, []),
     "cr_plan_columns": (ctypes.c_int, [ctypes.POINTER(CrBatch), ctypes.c_double, ctypes.c_double,
-                                       ctypes.c_void_p]),
+                                       ctypes.c_double, ctypes.c_void_p]),
     "cr_march_static": (ctypes.c_int, [ctypes.POINTER(CrBatch), ctypes.POINTER(CrOutputs), ctypes.c_void_p]),
     "cr_cell_tl": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                   ctypes.c_void_p]),

@@ -1192,29 +1192,39 @@ double operator_changes(const cr_batch* b, const cr_ray& r) {
 struct MarchCosts {
     double row_step_s = 0.0;     // one batched tile alone: one row of one step
     double updates_per_s = 0.0;  // batched kernel over a device-filling batch
+    double slots = 0.0;          // batched tiles the device holds at once
 };
 
 // The cost rule of the column policy.  A ray's lockstep march in a batched
 // tile takes about (nz + 2)(nr + 4 + 4 x operator changes) row steps of one
 // warp in sequence; when that alone exceeds the time the whole batch needs at
 // the batched kernel's throughput by the margin, the ray would set the
-// launch's length, and a cluster of SMs marches it instead.
+// launch's length, and a cluster of SMs marches it instead.  A row step
+// takes the tile's own time alone, or longer when the rays in flight together
+// - the batch's, up to what the device's tile slots hold - would exceed the
+// batched throughput at that pace.
 std::vector<char> cost_rule(const cr_batch* b, const MarchCosts& c) {
     // a ray leaves the batched kernel only when it would clearly outlast the
     // batch: in a homogeneous batch every ray's march is close to the
     // balanced time, and the batched kernel is the efficient one there
     constexpr double kMargin = 1.25;
     std::vector<char> col((size_t)b->n_rays, 0);
-    double work = 0.0;
-    for (int i = 0; i < b->n_rays; ++i) work += (double)b->rays[i].nz * b->rays[i].nr;
+    double work = 0.0, per_tile = 0.0;
+    for (int i = 0; i < b->n_rays; ++i) {
+        work += (double)b->rays[i].nz * b->rays[i].nr;
+        per_tile += (double)(kTile / ((b->rays[i].np + crk::kT - 1) / crk::kT));
+    }
+    per_tile /= std::max(1, b->n_rays);
     const double tau = work / c.updates_per_s;
+    const double in_flight = c.slots > 0.0 ? std::min((double)b->n_rays, c.slots * per_tile) : (double)b->n_rays;
+    const double row = std::max(c.row_step_s, in_flight / c.updates_per_s);
     for (int i = 0; i < b->n_rays; ++i) {
         const cr_ray& r = b->rays[i];
         // every operator change (bathymetry index, profile update) costs the
         // batched march about four more passes: back-substitution alone, two
         // factorisation passes, elimination alone
         const double steps = (double)(r.nr + 4) + 4.0 * operator_changes(b, r);
-        col[(size_t)i] = (double)(r.nz + 2) * steps * c.row_step_s > kMargin * tau;
+        col[(size_t)i] = (double)(r.nz + 2) * steps * row > kMargin * tau;
     }
     return col;
 }
@@ -1322,6 +1332,7 @@ int cr_create(const cr_batch* b, cr_engine** out) {
         const std::vector<char> is_col = pick_column_rays(b, e->pd_n, b->precision, e->device, &costs);
         e->st.tuner_row_step_s = costs.row_step_s;
         e->st.tuner_updates_per_s = costs.updates_per_s;
+        e->st.tuner_slots = costs.slots;
         // batched rays grouped by Pade order, then work; a tile holds
         // floor(32/G) rays of G lanes each, G = the largest np in the tile
         std::vector<int> bord;
@@ -1923,7 +1934,7 @@ void cr_destroy(cr_engine* e) {
     delete e;
 }
 
-int cr_plan_columns(const cr_batch* b, double row_step_s, double updates_per_s, int32_t* is_column) {
+int cr_plan_columns(const cr_batch* b, double row_step_s, double updates_per_s, double slots, int32_t* is_column) {
     const std::string msg = validate(b);
     if (!msg.empty() || !is_column || !(row_step_s > 0.0) || !(updates_per_s > 0.0)) {
         set_global_error("cr_plan_columns: %s", msg.empty() ? "invalid arguments" : msg.c_str());
@@ -1932,6 +1943,7 @@ int cr_plan_columns(const cr_batch* b, double row_step_s, double updates_per_s, 
     MarchCosts c;
     c.row_step_s = row_step_s;
     c.updates_per_s = updates_per_s;
+    c.slots = slots;
     const std::vector<char> col = cost_rule(b, c);
     for (int i = 0; i < b->n_rays; ++i) is_column[i] = col[(size_t)i];
     return CR_OK;
@@ -1941,15 +1953,16 @@ int cr_plan_columns(const cr_batch* b, double row_step_s, double updates_per_s, 
 
 namespace {
 
-// The engine's own tuner: the two costs of the column policy, measured once
-// per device and precision form by marching a synthetic batch through the
-// engine itself (every ray on the batched kernel): two rounds of tiles for
-// every resident slot of the device (10 rays of np 6 per tile, nz 200, 40
-// steps).  Its time gives the batched throughput in grid-point updates/s,
-// and - a round being one lockstep tile march per slot - the time of one row
-// of one step of a tile under that load.  About 0.1 s on first use;
-// CUPYRAM_B200_COSTS="row_step_s,updates_per_s" sets both instead
-// (reproducible schedules).
+// The engine's own tuner: the costs of the column policy, measured once per
+// device and precision form by marching synthetic batches through the engine
+// itself (every ray on the batched kernel):
+//   * one tile alone (10 rays of np 6, nz 2000, 30 steps): the time of one
+//     row of one step of a lockstep tile when nothing else runs;
+//   * two rounds of tiles for every resident slot of the device (nz 200,
+//     40 steps): the batched throughput in grid-point updates/s, and the slots
+//     (the CTAs of the persistent launch).
+// About 0.1 s on first use; CUPYRAM_B200_COSTS="row_step_s,updates_per_s,slots"
+// sets them instead (reproducible schedules).
 std::mutex g_costs_mu;
 std::map<std::pair<int, int>, MarchCosts> g_costs;
 
@@ -2024,7 +2037,8 @@ double synth_march_ms(int n_rays, int nz, int nr, int precision, int* ctas) {
 MarchCosts march_costs(int device, int precision) {
     MarchCosts c;
     if (const char* v = getenv("CUPYRAM_B200_COSTS")) {
-        if (sscanf(v, "%lf,%lf", &c.row_step_s, &c.updates_per_s) == 2 && c.row_step_s > 0 && c.updates_per_s > 0)
+        if (sscanf(v, "%lf,%lf,%lf", &c.row_step_s, &c.updates_per_s, &c.slots) >= 2 && c.row_step_s > 0 &&
+            c.updates_per_s > 0)
             return c;
     }
     std::lock_guard<std::mutex> lock(g_costs_mu);
@@ -2034,18 +2048,19 @@ MarchCosts march_costs(int device, int precision) {
     // if a measurement fails: one B200's figures for the plain form
     c.row_step_s = 0.3e-6;
     c.updates_per_s = 1.3e10;
+    c.slots = 0.0;
     g_in_tuner = true;
     {
-        int sms = 148, ctas = 0;
+        int sms = 148, ctas = 0, ctas1 = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        const int nz1 = 2000, nr1 = 30;
+        const double t1 = synth_march_ms(10, nz1, nr1, precision, &ctas1);
         const int nz = 200, nr = 40, rays = 10 * 2 * 7 * sms;
         const double t = synth_march_ms(rays, nz, nr, precision, &ctas);
-        if (t > 0.0 && ctas > 0) {
-            const double tiles = (double)rays / 10.0;
-            c.updates_per_s = (double)rays * nz * nr / (t * 1e-3);
-            // a march without operator changes takes about nr + 12 row sweeps
-            c.row_step_s = t * 1e-3 * (double)ctas / tiles / ((double)(nz + 2) * (double)(nr + 12));
-        }
+        // a march without operator changes takes about nr + 12 row sweeps
+        if (t1 > 0.0) c.row_step_s = t1 * 1e-3 / ((double)(nz1 + 2) * (double)(nr1 + 12));
+        if (t > 0.0) c.updates_per_s = (double)rays * nz * nr / (t * 1e-3);
+        if (ctas > 0) c.slots = ctas;
     }
     g_in_tuner = false;
     // the tuner's engines leave their memory in the pool: hand it back

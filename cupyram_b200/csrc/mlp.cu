@@ -593,11 +593,11 @@ int grid_for(long long n) {
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 
-// CUPYRAM_B200_GEMM=tma selects the TMA-fed kernel for cr_mlp_gemm_tc
-// (default: the cp.async-fed one).
+// cr_mlp_gemm_tc feeds its operands by the tensor memory accelerator;
+// CUPYRAM_B200_GEMM=cp selects the kernel fed by per-thread cp.async.
 bool use_tma_gemm() {
     const char* v = getenv("CUPYRAM_B200_GEMM");
-    return v && v[0] == 't';
+    return !(v && v[0] == 'c');
 }
 
 // cuTensorMapEncodeTiled, reached through the runtime's driver entry point

@@ -133,7 +133,7 @@ class Engine:
             pass
 
 
-def plan_columns(batch: Batch, row_step_s, updates_per_s):
+def plan_columns(batch: Batch, row_step_s, updates_per_s, slots=0):
     """The column policy's cost rule for given costs (cr_plan_columns, host only):
     a bool array, True for the rays whose lockstep march in a batched tile
     would outlast the whole batch's balanced time by the policy's margin."""
@@ -149,7 +149,8 @@ def plan_columns(batch: Batch, row_step_s, updates_per_s):
     desc.compute_grids = 1 if batch.compute_grids else 0
     desc.line_len, desc.grid_len = batch.line_len, batch.grid_len
     out = np.zeros(len(rays), np.int32)
-    _lib.check(lib.cr_plan_columns(ctypes.byref(desc), float(row_step_s), float(updates_per_s), out.ctypes.data))
+    _lib.check(lib.cr_plan_columns(ctypes.byref(desc), float(row_step_s), float(updates_per_s), float(slots),
+                                   out.ctypes.data))
     return out.astype(bool)
 
 

@@ -149,6 +149,7 @@ typedef struct cr_stats {
                                  one row of one step of a tile alone (0: the
                                  policy was forced by CUPYRAM_B200_COL)         */
     double tuner_updates_per_s; /* measured batched throughput it used          */
+    double tuner_slots;       /* batched tiles the device holds at once         */
 } cr_stats;
 
 typedef struct cr_engine cr_engine;
@@ -241,14 +242,16 @@ void cr_destroy(cr_engine* e);
 /*
  * The cost rule the engine's column policy applies at cr_create, on the host:
  * is_column[i] = 1 when ray i's lockstep march in a batched tile,
- * (nz + 2)(nr + 4 + 4 x operator changes) x row_step_s, exceeds 1.25 x the
- * whole batch's balanced time, sum(nz nr) / updates_per_s.  cr_create takes
- * both costs from the engine's tuner (measured once per device and precision
- * form; cr_stats.tuner_*), and sends a chosen ray to the column kernel when
- * its column also fits a cluster.  No counterpart in the reference, which
- * sizes one grid for all rays (cupyram/cupyram.py:596-597).
+ * (nz + 2)(nr + 4 + 4 x operator changes) x row, exceeds 1.25 x the whole
+ * batch's balanced time, sum(nz nr) / updates_per_s.  row is the larger of
+ * row_step_s (a tile alone) and in_flight / updates_per_s, in_flight being
+ * the batch's rays, at most slots x the mean rays per tile (slots <= 0: no
+ * cap).  cr_create takes the costs from the engine's tuner (measured once per
+ * device and precision form; cr_stats.tuner_*), and sends a chosen ray to the
+ * column kernel when its column also fits a cluster.  No counterpart in the
+ * reference, which sizes one grid for all rays (cupyram/cupyram.py:596-597).
  */
-int cr_plan_columns(const cr_batch* batch, double row_step_s, double updates_per_s,
+int cr_plan_columns(const cr_batch* batch, double row_step_s, double updates_per_s, double slots,
                     int32_t* is_column);
 
 /*

@@ -47,11 +47,11 @@ def test_gemm_epilogues_vs_numpy(cuda_device):
 def test_gemm_tcgen05_vs_numpy(cuda_device, monkeypatch, feed, M, N, K):
     """The tcgen05 kernels (accumulator in tensor memory) on every epilogue, and their wait
     flag clear: operands fed by per-thread cp.async, or by the tensor memory accelerator
-    with a producer warp and an MMA warp (CUPYRAM_B200_GEMM=tma; K of 192 and 640 run
-    the two-stage ring through 3 and 10 tiles)."""
+    with a producer warp and an MMA warp (the default; CUPYRAM_B200_GEMM=cp selects the
+    other; K of 192 and 640 run the two-stage ring through 3 and 10 tiles)."""
     import torch
     from cupyram_b200 import surrogate as S
-    monkeypatch.setenv("CUPYRAM_B200_GEMM", "tma" if feed == "tma" else "")
+    monkeypatch.setenv("CUPYRAM_B200_GEMM", "tma" if feed == "tma" else "cp")
     rng = np.random.default_rng(4)
     A, B = rng.normal(size=(M, K)), rng.normal(size=(N, K))
     bias = rng.normal(size=N)
