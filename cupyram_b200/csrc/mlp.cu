@@ -593,11 +593,180 @@ int grid_for(long long n) {
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 
-// cr_mlp_gemm_tc feeds its operands by the tensor memory accelerator;
-// CUPYRAM_B200_GEMM=cp selects the kernel fed by per-thread cp.async.
-bool use_tma_gemm() {
+// The kernel behind cr_mlp_gemm_tc: the persistent TMA-fed one by default;
+// CUPYRAM_B200_GEMM=tma the one-block-per-CTA TMA-fed one, =cp the one fed by
+// per-thread cp.async.
+int gemm_feed() {
     const char* v = getenv("CUPYRAM_B200_GEMM");
-    return !(v && v[0] == 'c');
+    if (v && v[0] == 'c') return 0;
+    if (v && v[0] == 't') return 1;
+    return 2;
+}
+
+// ---------------------------------------------------------------------------
+// Persistent TMA-fed tcgen05 contraction with the epilogue overlapped.
+//
+// One CTA per SM walks the output blocks (128 x 256) in a static round
+// robin.  Six warps:
+//   * warp 0, lane 0: TMA producer over a kPStages-deep ring of stages;
+//   * warp 1, lane 0: MMA issuer, accumulating block i in one of two TMEM
+//     accumulators (columns 0..255 or 256..511, by i's parity), committing
+//     each stage to its "empty" barrier and each finished block to its
+//     accumulator's "full" barrier;
+//   * warps 2..5: the epilogue, one TMEM lane quadrant each (quadrant =
+//     warp mod 4), reading block i's accumulator while the MMAs of block i+1
+//     run in the other one, then releasing it on its "empty" barrier.
+// Every wait is bounded; a role that gives up stops, the CTA sets *err, and
+// the output is incomplete.
+// ---------------------------------------------------------------------------
+constexpr int kPStages = 4;
+constexpr int kPThreads = 192;
+constexpr size_t kPSmem = (size_t)kPStages * kUStage + (size_t)4 * 32 * 33 * 4 + 1024 + 512;
+
+template <int EPI>
+__global__ void __launch_bounds__(kPThreads, 1) gemm_tn_persistent(const __grid_constant__ CUtensorMap mapA,
+                                                                   const __grid_constant__ CUtensorMap mapB, int M,
+                                                                   int N, int K, EpiArgs e, int* err) {
+    extern __shared__ __align__(1024) unsigned char usmem[];
+    unsigned char* base = (unsigned char*)(((uintptr_t)usmem + 1023) & ~(uintptr_t)1023);
+    auto tA = [&](int st) { return base + st * kUStage; };
+    auto tB = [&](int st) { return base + st * kUStage + kUTileA; };
+    float* stg_all = reinterpret_cast<float*>(base + kPStages * kUStage);
+    uint64_t* full = (uint64_t*)(base + kPStages * kUStage + 4 * 32 * 33 * 4);
+    uint64_t* empty = full + kPStages;
+    uint64_t* acc_full = empty + kPStages;   // [2]
+    uint64_t* acc_empty = acc_full + 2;      // [2]
+    uint32_t* taddr_s = (uint32_t*)(acc_empty + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nk = K / UBK, nbm = M / UBM, nbn = N / UBN, nblocks = nbm * nbn;
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(taddr_s)),
+                     "r"(2 * UBN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 32) {
+        for (int s = 0; s < kPStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(&acc_full[a], 1);
+            mbar_init(&acc_empty[a], 4);  // one arrival per epilogue warp
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *taddr_s;
+    bool ok = true;
+    int issued = 0;  // producer: k-tiles whose loads were issued (over all blocks)
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int g = 0;
+            for (int blk = blockIdx.x; blk < nblocks && ok; blk += gridDim.x) {
+                const int bm = (blk % nbm) * UBM, bn = (blk / nbm) * UBN;
+                for (int kt = 0; kt < nk && ok; ++kt, ++g) {
+                    const int st = g % kPStages;
+                    if (g >= kPStages) ok &= mbar_wait(&empty[st], ((g / kPStages) - 1) & 1);
+                    if (!ok) break;
+                    mbar_expect_tx(&full[st], (unsigned)kUStage);
+                    tma_load_2d(tA(st), &mapA, kt * UBK, bm, &full[st]);
+                    tma_load_2d(tB(st), &mapB, kt * UBK, bn, &full[st]);
+                    issued = g + 1;
+                }
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int g = 0, i = 0;
+            for (int blk = blockIdx.x; blk < nblocks && ok; blk += gridDim.x, ++i) {
+                const int a = i & 1;
+                // the epilogue has drained this accumulator's previous block
+                if (i >= 2) ok &= mbar_wait(&acc_empty[a], ((i / 2) - 1) & 1);
+                if (!ok) break;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t acc_addr = tmem + (uint32_t)(a * UBN);
+                for (int kt = 0; kt < nk && ok; ++kt, ++g) {
+                    const int st = g % kPStages;
+                    ok &= mbar_wait(&full[st], (g / kPStages) & 1);
+                    if (!ok) break;
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t sa = smem_u32(tA(st)), sb = smem_u32(tB(st));
+#pragma unroll
+                    for (int k = 0; k < UBK / 16; ++k) {
+                        const uint64_t da = umma_desc_sw128(sa + k * 32), db = umma_desc_sw128(sb + k * 32);
+                        const uint32_t accum = (kt > 0 || k > 0) ? 1u : 0u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+                            :
+                            : "r"(acc_addr), "l"(da), "l"(db), "r"(kUIdesc), "r"(accum)
+                            : "memory");
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                     smem_u32(&empty[st]))
+                                 : "memory");
+                }
+                if (!ok) break;
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&acc_full[a]))
+                             : "memory");
+            }
+        }
+    } else {
+        // epilogue: TMEM lane quadrant q = warp mod 4 holds rows 32q..32q+31
+        const int q = warp & 3;
+        float* stg = stg_all + (warp - 2) * 32 * 33;
+        int i = 0;
+        for (int blk = blockIdx.x; blk < nblocks && ok; blk += gridDim.x, ++i) {
+            const int a = i & 1;
+            const int bm = (blk % nbm) * UBM, bn = (blk / nbm) * UBN;
+            ok &= mbar_wait(&acc_full[a], (i / 2) & 1);
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+            for (int cc = 0; cc < UBN; cc += 32) {
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    uint32_t v[16];
+                    const uint32_t ta = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * UBN + cc + 16 * h);
+                    asm volatile(
+                        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,"
+                        "%15}, [%16];"
+                        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                          "=r"(v[14]), "=r"(v[15])
+                        : "r"(ta));
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) stg[lane * 33 + 16 * h + j] = __uint_as_float(v[j]);
+                }
+                __syncwarp();
+#pragma unroll 4
+                for (int r = 0; r < 32; ++r) store1<EPI>(e, bm + q * 32 + r, bn + cc + lane, stg[r * 33 + lane]);
+                __syncwarp();
+            }
+            // this warp's reads of the accumulator are done: release it to the MMAs
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[a])) : "memory");
+        }
+    }
+    __syncwarp();
+    ok = __syncthreads_and(ok ? 1 : 0) != 0;
+    if (!ok && warp == 0 && lane == 0) {
+        // no copy may still be writing this CTA's shared memory when it exits
+        for (int g = issued - 1; g >= 0 && g >= issued - kPStages; --g)
+            mbar_wait(&full[g % kPStages], (g / kPStages) & 1);
+    }
+    if (!ok && tid == 0) atomicExch(err, 1);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * UBN));
 }
 
 // cuTensorMapEncodeTiled, reached through the runtime's driver entry point
@@ -673,7 +842,34 @@ int cr_mlp_gemm_tc(int epi, const void* A, const void* B, int M, int N, int K, i
     auto a = (const __nv_bfloat16*)A;
     auto b = (const __nv_bfloat16*)B;
     cudaError_t ce = cudaSuccess;
-    if (use_tma_gemm()) {
+    const int feed = gemm_feed();
+    if (feed == 2) {
+        // persistent: one CTA per SM, operands by the tensor memory accelerator
+        CUtensorMap ma, mb;
+        if (!operand_map(&ma, A, M, K, lda, UBM) || !operand_map(&mb, B, N, K, ldb, UBN)) return CR_MLP_ECUDA;
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            return CR_MLP_ECUDA;
+        const int blocks = (M / UBM) * (N / UBN);
+        const int ctas = blocks < sms ? blocks : sms;
+        switch (epi) {
+#define CR_PERS_CASE(E)                                                                                          \
+    case E:                                                                                                      \
+        ce = cudaFuncSetAttribute(gemm_tn_persistent<E>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPSmem); \
+        if (ce == cudaSuccess) gemm_tn_persistent<E><<<ctas, kPThreads, kPSmem, st>>>(ma, mb, M, N, K, e, err);    \
+        break;
+            CR_PERS_CASE(CR_MLP_EPI_BIAS_RELU_BF16)
+            CR_PERS_CASE(CR_MLP_EPI_BIAS_F32)
+            CR_PERS_CASE(CR_MLP_EPI_F32)
+            CR_PERS_CASE(CR_MLP_EPI_RELU_MASK_BF16)
+#undef CR_PERS_CASE
+            default: return CR_MLP_EBADSHAPE;
+        }
+        if (ce != cudaSuccess) return CR_MLP_ECUDA;
+        return cudaGetLastError() == cudaSuccess ? 0 : CR_MLP_ECUDA;
+    }
+    if (feed == 1) {
         // operands by the tensor memory accelerator (tensor maps over this GPU's memory)
         CUtensorMap ma, mb;
         if (!operand_map(&ma, A, M, K, lda, UBM) || !operand_map(&mb, B, N, K, ldb, UBN)) return CR_MLP_ECUDA;

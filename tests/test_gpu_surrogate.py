@@ -42,16 +42,19 @@ def test_gemm_epilogues_vs_numpy(cuda_device):
         S.gemm(S.EPI_F32, _bf(A[:100]), Bb, out)  # M not a multiple of 128
 
 
-@pytest.mark.parametrize("feed,M,N,K", [("cp.async", 256, 512, 192), ("tma", 256, 512, 192),
-                                         ("tma", 384, 768, 640)])
+@pytest.mark.parametrize("feed,M,N,K", [("cp", 256, 512, 192), ("tma", 256, 512, 192), ("tma", 384, 768, 640),
+                                         ("persistent", 256, 512, 192), ("persistent", 384, 768, 640),
+                                         ("persistent", 2560, 38 * 256, 128)])
 def test_gemm_tcgen05_vs_numpy(cuda_device, monkeypatch, feed, M, N, K):
     """The tcgen05 kernels (accumulator in tensor memory) on every epilogue, and their wait
-    flag clear: operands fed by per-thread cp.async, or by the tensor memory accelerator
-    with a producer warp and an MMA warp (the default; CUPYRAM_B200_GEMM=cp selects the
-    other; K of 192 and 640 run the two-stage ring through 3 and 10 tiles)."""
+    flag clear: operands fed by per-thread cp.async (CUPYRAM_B200_GEMM=cp), by the tensor
+    memory accelerator one block per CTA (=tma), or by the persistent kernel (the default:
+    one CTA per SM, a TMA producer warp, an MMA warp and four epilogue warps overlapping
+    two tensor-memory accumulators).  K of 192 and 640 run a ring through 3 and 10 tiles;
+    20 x 38 blocks give every CTA of the persistent kernel several blocks."""
     import torch
     from cupyram_b200 import surrogate as S
-    monkeypatch.setenv("CUPYRAM_B200_GEMM", "tma" if feed == "tma" else "cp")
+    monkeypatch.setenv("CUPYRAM_B200_GEMM", {"cp": "cp", "tma": "tma", "persistent": ""}[feed])
     rng = np.random.default_rng(4)
     A, B = rng.normal(size=(M, K)), rng.normal(size=(N, K))
     bias = rng.normal(size=N)
