@@ -441,9 +441,9 @@ def run_gemm(a):
     flop = 2.0 * M * N * K
     peak, kind = measured_peak_bf16()
     res = {}
-    for name, tc, feed in (("tcgen05 persistent (TMA-fed, overlapped epilogue)", True, ""),
-                           ("tcgen05 (TMA-fed)", True, "tma"), ("tcgen05 (cp.async-fed)", True, "cp"),
-                           ("mma.sync", False, "cp")):
+    for name, tc, feed in (("tcgen05 (TMA-fed)", True, ""),
+                           ("tcgen05 persistent (TMA-fed, overlapped epilogue)", True, "persistent"),
+                           ("tcgen05 (cp.async-fed)", True, "cp"), ("mma.sync", False, "cp")):
         os.environ["CUPYRAM_B200_GEMM"] = feed
         for _ in range(a.warmup):
             S.gemm(S.EPI_BIAS_F32, A, B, out, bias=bias, tc=tc)
@@ -458,10 +458,10 @@ def run_gemm(a):
         res[name] = {"ms": ms, "tflops": flop / ms * 1e-9}
     assert int(S.tc_error_flag().item()) == 0
     os.environ.pop("CUPYRAM_B200_GEMM", None)
-    t = res["tcgen05 persistent (TMA-fed, overlapped epilogue)"]["tflops"]
+    t = res["tcgen05 (TMA-fed)"]["tflops"]
     line = {"metric": "surrogate GEMM TFLOP/s (bf16 x bf16 -> f32, 8192 x 8192 x 512)", "value": t,
             "unit": "TFLOP/s", "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
-            "ms_per_step": res["tcgen05 persistent (TMA-fed, overlapped epilogue)"]["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": res["tcgen05 (TMA-fed)"]["ms"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "bf16", "data": "synthetic (random matrices)",
             "config": {"workload": "surrogate last-layer contraction, batch of 8192 requests", "config": "gemm",
                        "l2": "operands 16 MB (L2-resident); output 268 MB"},

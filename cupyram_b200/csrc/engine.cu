@@ -1247,7 +1247,12 @@ std::vector<char> pick_column_rays(const cr_batch* b, const std::vector<int>& pd
     std::vector<char> want((size_t)b->n_rays, 1);
     if (mode == 2) {
         *used = march_costs(device, precision);
-        want = cost_rule(b, *used);
+        // the rule paces the tiles by all the batch's rays in flight: capping
+        // them at the device's tile slots kept 150 more wedge rays batched
+        // and measured slower (11.7 s against 9.4 s)
+        MarchCosts c = *used;
+        c.slots = 0.0;
+        want = cost_rule(b, c);
     }
     std::map<std::tuple<int, int, int>, bool> runs;
     for (int i = 0; i < b->n_rays; ++i) {

@@ -48,13 +48,13 @@ def test_gemm_epilogues_vs_numpy(cuda_device):
 def test_gemm_tcgen05_vs_numpy(cuda_device, monkeypatch, feed, M, N, K):
     """The tcgen05 kernels (accumulator in tensor memory) on every epilogue, and their wait
     flag clear: operands fed by per-thread cp.async (CUPYRAM_B200_GEMM=cp), by the tensor
-    memory accelerator one block per CTA (=tma), or by the persistent kernel (the default:
-    one CTA per SM, a TMA producer warp, an MMA warp and four epilogue warps overlapping
-    two tensor-memory accumulators).  K of 192 and 640 run a ring through 3 and 10 tiles;
+    memory accelerator one block per CTA (the default), or by the persistent kernel
+    (=persistent: one CTA per SM, a TMA producer warp, an MMA warp and four epilogue warps
+    overlapping two tensor-memory accumulators).  K of 192 and 640 run a ring through 3 and 10 tiles;
     20 x 38 blocks give every CTA of the persistent kernel several blocks."""
     import torch
     from cupyram_b200 import surrogate as S
-    monkeypatch.setenv("CUPYRAM_B200_GEMM", {"cp": "cp", "tma": "tma", "persistent": ""}[feed])
+    monkeypatch.setenv("CUPYRAM_B200_GEMM", {"cp": "cp", "tma": "", "persistent": "persistent"}[feed])
     rng = np.random.default_rng(4)
     A, B = rng.normal(size=(M, K)), rng.normal(size=(N, K))
     bias = rng.normal(size=N)
