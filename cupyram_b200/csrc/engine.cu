@@ -1728,6 +1728,8 @@ int cr_march(cr_engine* e) {
         sa.cpg = e->d_cpg;
         sa.flags = e->d_flags;
         sa.compute_grids = e->compute_grids;
+        if (e->n_tiles > 0 && !crk::encode_sum_maps(sa, e->precision, e->col_elems / kTile, e->lane_elems / kTile))
+            return e->fail(CR_ECUDA, "cr_march: the driver's tensor-map encoder is unavailable or refused a map");
         crk::ColArgs ca;
         ca.rays = e->d_rays;
         ca.col_ray = e->d_col_ray;
@@ -1812,10 +1814,15 @@ int cr_march(cr_engine* e) {
     std::vector<int> fl(e->n_rays);
     ce = cudaMemcpy(fl.data(), e->d_flags, fl.size() * sizeof(int), cudaMemcpyDeviceToHost);
     if (ce != cudaSuccess) return e->cuda_fail(ce, "cr_march (flags)");
-    int failed = 0;
-    for (int v : fl) failed += (v != 0);
+    int failed = 0, timed_out = 0;
+    for (int v : fl) {
+        failed += (v != 0);
+        timed_out += (v & 2) != 0;
+    }
     e->st.rays_failed = failed;
     e->marched = true;
+    if (timed_out)
+        return e->fail(CR_ETIMEOUT, "%d ray(s): a wait for the march's bulk copies gave up", timed_out);
     if (failed) return e->fail(CR_ENAN, "%d ray(s) produced a non-finite field", failed);
     return CR_OK;
 }

@@ -298,6 +298,46 @@ __device__ __forceinline__ void cp_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
+// ---------------------------------------------------------------------------
+// Bulk tensor copies (cp.async.bulk.tensor, no multicast) completing on an
+// mbarrier in shared memory
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void mbar_init1(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+// arrive once and expect `bytes` more bytes of copies on the current phase
+__device__ __forceinline__ void mbar_expect(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// true once the phase of this parity has completed; false after `limit` polls
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, unsigned limit) {
+    for (unsigned it = 0; it < limit; ++it) {
+        unsigned done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+// one box of a 2-D tensor map (map: address of a CUtensorMap in parameter,
+// constant or global memory) at element coordinates (x, y) into shared memory
+__device__ __forceinline__ void tma_2d(void* dst, const void* map, int x, int y, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(smem_u32(dst)),
+        "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+// orders this thread's earlier generic-proxy accesses before later
+// async-proxy (bulk copy) accesses, in global and shared memory
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async;" ::: "memory"); }
+
 struct EnvRow {
     float f1, f2, f3;
     float2 k;

@@ -4,9 +4,56 @@
 // march_sum_impl.cuh).
 #include <cuda_runtime.h>
 
+#include <cstring>
+
 #include "march_sum.cuh"
+#include "tensor_map.h"
 
 namespace crk {
+
+namespace {
+
+// Map of an array stored as rows of 32 elements of elem_bytes bytes (rows
+// rows), viewed as 8-byte words, in boxes of the first `cols` elements of
+// kRB rows: plain tiles, no swizzle, no interleave, zeros outside the array.
+// Boxes narrower than a row (the ray columns of a tile) take no L2
+// promotion: a wider fetch would read the unused columns from DRAM.
+bool rows_map(EncodeTiledFn enc, CUtensorMap* m, const void* base, int elem_bytes, long long rows, int cols) {
+    const cuuint64_t dims[2] = {(cuuint64_t)(kTile * elem_bytes / 8), (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)(kTile * elem_bytes)};
+    const cuuint32_t box[2] = {(cuuint32_t)(cols * elem_bytes / 8), (cuuint32_t)kRB};
+    const cuuint32_t estr[2] = {1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_UINT64, 2, const_cast<void*>(base), dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               cols == kTile ? CU_TENSOR_MAP_L2_PROMOTION_L2_256B : CU_TENSOR_MAP_L2_PROMOTION_NONE,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+}  // namespace
+
+bool encode_sum_maps(SumArgs& a, int form, long long ray_rows, long long lane_rows) {
+    std::memset(&a.maps, 0, sizeof a.maps);
+    const EncodeTiledFn enc = encode_tiled();
+    if (!enc || ray_rows <= 0 || lane_rows <= 0) return false;
+    const int vb = form == CR_PLAIN_C128 ? 16 : 8;  // factors and workspace: complex128 or complex64
+    const int eb = form == CR_CHOSEN_C64 ? 8 : 16;  // couplings
+    const void* lanes[5];
+    lanes[kMapG] = a.G;
+    lanes[kMapQD] = a.QD;
+    lanes[kMapWD] = a.WD;
+    lanes[kMapQU] = a.QU;
+    lanes[kMapWU] = a.WU;
+    bool ok = true;
+    for (int i = 0; i < 5; ++i) ok = ok && rows_map(enc, &a.maps.lane[i], lanes[i], vb, lane_rows, kTile);
+    for (int P = 1; P <= kMaxP; ++P) {
+        const int R = kTile / P;  // rays of a tile whose rays take P lanes
+        ok = ok && rows_map(enc, &a.maps.ray[kMapU][P - 1], a.u, 16, ray_rows, R);
+        ok = ok && rows_map(enc, &a.maps.ray[kMapED][P - 1], a.ED, eb, ray_rows, R);
+        ok = ok && rows_map(enc, &a.maps.ray[kMapEU][P - 1], a.EU, eb, ray_rows, R);
+        if (a.E2) ok = ok && rows_map(enc, &a.maps.ray[kMapE2][P - 1], a.E2, 16, ray_rows, R);
+    }
+    return ok;
+}
 
 cudaError_t sum_launch_plain(const SumArgs& a, int p, int count, cudaStream_t st);
 cudaError_t sum_launch_chosen(const SumArgs& a, int p, int count, cudaStream_t st);

@@ -1,6 +1,8 @@
 // march_sum.cuh - launch interface of the partial-fraction (sum form) march.
 #pragma once
 
+#include <cuda.h>  // CUtensorMap
+
 #include "march_common.cuh"
 
 namespace crk {
@@ -10,6 +12,41 @@ namespace crk {
 #define CR_SUM_TERMS 2
 #endif
 constexpr int kT = CR_SUM_TERMS;
+
+// The solve passes stream their rows in blocks of kRB rows, one tensor copy
+// per field and block, through a ring of ring_blocks(form) blocks in shared
+// memory (complex128 form: CR_SUM_NB; complex64 forms: CR_SUM_NB_C64).
+#ifndef CR_SUM_RB
+#define CR_SUM_RB 8
+#endif
+#ifndef CR_SUM_NB
+#define CR_SUM_NB 2
+#endif
+#ifndef CR_SUM_NB_C64
+#define CR_SUM_NB_C64 CR_SUM_NB
+#endif
+constexpr int kRB = CR_SUM_RB;
+__host__ __device__ constexpr int ring_blocks(int form) { return form == 0 ? CR_SUM_NB : CR_SUM_NB_C64; }
+constexpr int kNBMax = CR_SUM_NB > CR_SUM_NB_C64 ? CR_SUM_NB : CR_SUM_NB_C64;
+
+// Largest lanes-per-ray value the kernels are instantiated for (np <= 10).
+constexpr int kMaxP = (10 + kT - 1) / kT;
+
+// Tensor maps of the solve passes' bulk copies (cp.async.bulk.tensor, 2-D,
+// 8-byte elements, no multicast).  Every map views one array as rows of the
+// 32 columns of a tile ([row][32], as stored) and copies boxes of kRB rows:
+//   lane[i]: G, QD, WD, QU, WU - all 32 lane columns of a row;
+//   ray[f][P-1]: u, ED, EU, E2 - the floor(32 / P) ray columns of a tile whose
+//   rays take P lanes each.
+// Row y of a map is element y * 32 of the array; a tile's rows start at
+// y = tile_off / 32 (ray arrays) and tile_loff / 32 + t * rows (term slot t of
+// the lane arrays).  Rows outside the array read as zeros.
+enum { kMapG = 0, kMapQD = 1, kMapWD = 2, kMapQU = 3, kMapWU = 4 };
+enum { kMapU = 0, kMapED = 1, kMapEU = 2, kMapE2 = 3 };
+struct SumMaps {
+    CUtensorMap lane[5];
+    CUtensorMap ray[4][kMaxP];
+};
 
 // Device pointers of one sum-form march.  Ray columns (f1..f3, ksq, u) and
 // lane columns (G and the factors) are stored [row][32] per tile, starting at
@@ -49,7 +86,14 @@ struct SumArgs {
     const int* queue;
     int n_queue;
     int max_ctas;  // persistent launch: CTAs = every resident slot (0), or this many
+    SumMaps maps;  // the kernels take SumArgs as a __grid_constant__ parameter
 };
+
+// Encodes a.maps for the arrays in a (G, QD, WD, QU, WU over lane_rows rows,
+// u, ED, EU and E2 over ray_rows rows; E2 only when not NULL) for the given
+// precision form.  Returns false when the driver's encoder is unavailable or
+// refuses a map.
+bool encode_sum_maps(SumArgs& a, int form, long long ray_rows, long long lane_rows);
 
 // form: an enum cr_precision value.  CR_PLAIN_C128: complex128 factors /
 // workspace and FP64 sweeps; CR_CHOSEN_C64R: complex64 factors / workspace
@@ -58,8 +102,6 @@ struct SumArgs {
 // couplings (ED / EU read as float2), M u and the term combination in FP32;
 // CR_C64_REFINED: as CR_CHOSEN_C64R with one FP64-residual refinement step per
 // term and range step (two passes per step; E2 holds the rows' d2).
-// Largest lanes-per-ray value the kernels are instantiated for (np <= 10).
-constexpr int kMaxP = (10 + kT - 1) / kT;
 // tile_P: host copy of tile_G.  One launch per run of equal P: run i goes
 // on streams[i % n_streams] (independent runs overlap); the number of
 // launches is returned in *launches.

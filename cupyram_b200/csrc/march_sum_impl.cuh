@@ -29,8 +29,11 @@
 // count), so the warp runs in lockstep.  The Thomas factorisation of each
 // term (1/den, the coupling factor and w per row, both directions) is
 // computed once per change of the operator - profiles, bathymetry index or
-// Pade set - and streamed from HBM, with the workspace g, through a per-lane
-// cp.async prefetch ring.  Only 1/den and w are stored per term; the
+// Pade set - and streamed from HBM, with the workspace g and the field, by
+// the tensor memory accelerator: one lane issues one bulk tensor copy per
+// field and block of kRB rows of the whole tile into a ring of blocks in
+// shared memory, completing on the block's mbarrier, which every lane waits
+// on before it reads the block.  Only 1/den and w are stored per term; the
 // elimination's coupling factor -(a1 + pd2 e) / den is rebuilt in FP64 from
 // 1/den and the row's Galerkin coupling e (d1 going down, d3 going up,
 // complex128), which is stored once per ray row and shared by the ray's
@@ -53,13 +56,16 @@ namespace crk {
 
 namespace {
 
-constexpr int kSR = 8;                // prefetch depth (rows) per lane
+constexpr int kSR = 8;                // factor passes: cp.async prefetch depth (rows) per lane
+constexpr unsigned kRingWaitLimit = 1u << 22;  // polls of a ring block's mbarrier before giving up
+static_assert((kRB & (kRB - 1)) == 0, "kRB must be a power of two");
 #ifndef CR_SUM_ROWS
 #define CR_SUM_ROWS 2
 #endif
 constexpr int kU = CR_SUM_ROWS;       // rows per solve-loop iteration
 static_assert((kSR & (kSR - 1)) == 0, "kSR must be a power of two");
 static_assert(kSR % kU == 0, "the prefetch ring must hold whole iterations");
+static_assert(kRB % kU == 0, "a ring block must hold whole iterations");
 
 enum SumPass { kElimOnly = 0, kFusedP = 1, kBackOnly = 2, kFactor = 3, kRefineUp = 4 };
 
@@ -75,28 +81,6 @@ enum SumPass { kElimOnly = 0, kFusedP = 1, kBackOnly = 2, kFactor = 3, kRefineUp
 // every form.
 constexpr int kPlain = 0, kChosen = 1, kFast = 2, kRefined = 3;
 
-// The prefetch ring in shared memory: [kSR rows][fields][32 lanes] of 16-byte
-// slots.  Fields: u, e, then (w, g, q) per term slot; the refined form adds
-// the row's d1 and d2 (its residual needs the whole Galerkin row).
-template <int F>
-__host__ __device__ constexpr int fields_of() {
-    return F == kRefined ? 4 + 3 * kT : 2 + 3 * kT;
-}
-template <int F>
-__host__ __device__ constexpr size_t smem_of() {
-    return (size_t)kSR * fields_of<F>() * kTile * sizeof(double2);
-}
-struct SumSmem {
-    double2 d[1];  // [kSR][fields_of<F>()][kTile]
-};
-template <int F>
-__device__ __forceinline__ double2* slot(SumSmem& S, int row, int field, int lane) {
-    return &S.d[(row * fields_of<F>() + field) * kTile + lane];
-}
-template <int F>
-__device__ __forceinline__ const double2* slot(const SumSmem& S, int row, int field, int lane) {
-    return &S.d[(row * fields_of<F>() + field) * kTile + lane];
-}
 template <int F>
 struct Form;
 template <>
@@ -128,6 +112,58 @@ struct Form<kFast> {
     using E = float2;
 };
 
+// Shared memory of a CTA (one warp), from its base:
+//   * the solve passes' ring: kNB blocks (ring_blocks of the form), each holding kRB rows of every field
+//     a solve pass streams, in 128-byte aligned regions (RingLayout<F>): the
+//     ray fields u, e (and d1, d2) as [kRB][floor(32 / P)] (the tile's rays),
+//     the lane fields w, g, q of each term slot as [kRB][32];
+//   * over the same bytes, the factor passes' cp.async ring, [kSR][2][32]
+//     16-byte slots (f1..f3 and ksq of each lane's ray row): a factor pass
+//     runs only between solve passes, whose copies have all landed;
+//   * after both, RingCtl: the ring's mbarriers and position.
+template <int F>
+struct RingLayout {
+    using V = typename Form<F>::V;
+    using E = typename Form<F>::E;
+    static constexpr int kRay = kRB * kTile * (int)sizeof(double2);  // u, d1, d2 (room for 32 rays)
+    static constexpr int kE = kRB * kTile * (int)sizeof(E);
+    static constexpr int kLane = kRB * kTile * (int)sizeof(V);
+    static constexpr int u = 0;
+    static constexpr int e = u + kRay;
+    static constexpr int w0 = e + kE;  // term slot t: w at w0 + 3 t kLane, then g, then q
+    static constexpr int d1 = w0 + 3 * kT * kLane;
+    static constexpr int d2 = d1 + kRay;
+    static constexpr int block = F == kRefined ? d2 + kRay : d1;
+    static constexpr int kNB = ring_blocks(F);
+    static_assert(kE % 128 == 0 && kLane % 128 == 0 && kRay % 128 == 0, "regions must stay 128-byte aligned");
+};
+struct RingCtl {
+    unsigned long long bar[kNBMax];  // one mbarrier per ring block (arrival count 1 + the copies' bytes)
+    unsigned seq;                    // ring blocks this CTA has consumed: slot seq % kNB, phase (seq / kNB) & 1
+    unsigned dead;                // a wait gave up: later waits are skipped and the CTA's rays are flagged
+};
+constexpr int kFactorRing = kSR * 2 * kTile * (int)sizeof(double2);
+template <int F>
+__host__ __device__ constexpr size_t ring_bytes() {
+    using Lay = RingLayout<F>;
+    return (size_t)(Lay::kNB * Lay::block > kFactorRing ? Lay::kNB * Lay::block : kFactorRing);
+}
+template <int F>
+__host__ __device__ constexpr size_t smem_of() {
+    return ring_bytes<F>() + sizeof(RingCtl);
+}
+struct SumSmem {
+    double2 d[1];
+};
+template <int F>
+__device__ __forceinline__ RingCtl* ring_ctl(SumSmem& S) {
+    return reinterpret_cast<RingCtl*>(reinterpret_cast<unsigned char*>(&S) + ring_bytes<F>());
+}
+template <int F>
+__device__ __forceinline__ unsigned char* ring_block(SumSmem& S, unsigned slot) {
+    return reinterpret_cast<unsigned char*>(&S) + slot * (unsigned)RingLayout<F>::block;
+}
+
 __device__ __forceinline__ double2 up2(double2 v) { return v; }
 __device__ __forceinline__ double2 up2(float2 v) { return make_double2((double)v.x, (double)v.y); }
 template <typename T>
@@ -158,6 +194,8 @@ struct Lane {
     int rows;               // rows per lane column, common to the warp (its deepest ray's nz + 2)
     int span;               // iterations per pass: rows rounded up to a multiple of kU
     int nzmin;              // shallowest ray of the warp (bounds the unchecked iterations)
+    int slot;               // the ray's index in the tile (its ray column)
+    int yray, ylane;        // first tensor-map row of the tile's ray columns / lane columns
     unsigned gmask;         // lanes of this ray
     unsigned wmask;         // active lanes of the warp: every pass runs in lockstep over them
     long long rcol;         // ray column base (f1..f3, ksq, u)
@@ -185,10 +223,11 @@ __device__ __forceinline__ typename Prec<R>::V* facw(double2* p) {
     return reinterpret_cast<typename Prec<R>::V*>(p);
 }
 
-template <int F>
-__device__ __forceinline__ float* sfl(SumSmem& S, int k, int lane) { return (float*)slot<F>(S, k, 0, lane); }
-template <int F>
-__device__ __forceinline__ float2* sks(SumSmem& S, int k, int lane) { return (float2*)slot<F>(S, k, 1, lane); }
+// factor-pass ring slots of prefetch row k: f1..f3 and ksq of the lane's ray row
+__device__ __forceinline__ float* sfl(SumSmem& S, int k, int lane) { return (float*)&S.d[(k * 2) * kTile + lane]; }
+__device__ __forceinline__ float2* sks(SumSmem& S, int k, int lane) {
+    return (float2*)&S.d[(k * 2 + 1) * kTile + lane];
+}
 
 // Stream row of iteration k: the same for every lane of the warp.
 template <bool DOWN>
@@ -202,11 +241,11 @@ template <int F, bool DOWN>
 __device__ __forceinline__ void sum_issue(const SumArgs& a, const Lane& L, SumSmem& S, int k, int r, int nz) {
     if (r >= 0 && r <= nz + 1) {
         const long long ro = L.rcol + (long long)r * kTile;
-        float* f = sfl<F>(S, k, L.lane);
+        float* f = sfl(S, k, L.lane);
         cp4(f + 0, a.f1 + ro);
         cp4(f + 1, a.f2 + ro);
         cp4(f + 2, a.f3 + ro);
-        cp8(sks<F>(S, k, L.lane), a.ksq + ro);
+        cp8(sks(S, k, L.lane), a.ksq + ro);
     }
     cp_commit();
 }
@@ -244,68 +283,48 @@ __device__ __forceinline__ PassPtrs<F> pass_ptrs(const SumArgs& a, const Lane& L
     return p;
 }
 
-template <typename T>
-__device__ __forceinline__ void cpt(void* dst, const void* src) {
-    if (sizeof(T) == 16) cp16(dst, src);
-    else cp8(dst, src);
-}
-template <typename T>
-__device__ __forceinline__ void cptz(void* dst, const void* src, bool on) {
-    if (sizeof(T) == 16) cp16z(dst, src, on);
-    else cp8z(dst, src, on);
-}
-
-// Copies for stream row r of a solve pass (one commit group).  The
-// elimination works two rows behind the stream (row m = r -/+ 2).  CHECK:
-// rows outside the lane's column are copied with zero source size (no
-// global read; the slot is zero-filled).  Without CHECK every row involved
-// is an interior row of every ray of the warp.
-template <int F, int PASS, bool DOWN, bool CHECK>
-__device__ __forceinline__ void solve_issue(const PassPtrs<F>& p, const Lane& L, SumSmem& S, int ks, int r,
-                                            int nz) {
+// Lane 0: the bulk tensor copies of block b of a solve pass into ring slot
+// `slot`, completing on the slot's mbarrier with the bytes it announces.  The
+// block's stream iterations b kRB .. b kRB + kRB - 1 cover the memory rows
+// lo .. lo + kRB - 1 (ascending in a DOWN pass, descending in an UP pass); the
+// elimination's rows (e, q; d1 and d2 of the residual pass) lie two rows
+// behind the stream, one in the refined form's residual pass.  Rows past the
+// tile's own belong to neighbouring tiles or read as zeros outside the array:
+// they are never used (the CHECK iterations select them away).
+template <int F, int P, int PASS, bool DOWN>
+__device__ __forceinline__ void ring_issue(const SumArgs& a, const Lane& L, SumSmem& S, int b, unsigned slot) {
+    using Lay = RingLayout<F>;
     using V = typename Form<F>::V;
     using E = typename Form<F>::E;
-    const bool on = CHECK ? ((r >= 0) & (r <= nz + 1)) : true;
-    const int ro = (CHECK ? (on ? r : 0) : r) * kTile;
-    // the refined form's residual pass needs u in every lane of the ray
-    const bool uon = (PASS == kElimOnly || PASS == kRefineUp) ? on : (on & (L.k == 0));
-    if (CHECK || PASS != kElimOnly) cp16z(slot<F>(S, ks, 0, L.lane), p.u + ro, uon);
-    else cp16(slot<F>(S, ks, 0, L.lane), p.u + ro);
-    // elimination row: two rows behind the stream; one row behind in the
-    // refined form's residual pass (UP)
-    const int m = PASS == kRefineUp ? r + 1 : (DOWN ? r - 2 : r + 2);
-    const bool mon = CHECK ? (on & (m >= 1) & (m <= nz)) : true;
-    const int mo = (CHECK ? (mon ? m : 0) : m) * kTile;
-    if constexpr (PASS == kRefineUp) {
-        if (CHECK) {
-            cp16z(slot<F>(S, ks, 2 + 3 * kT, L.lane), p.d1 + mo, mon);
-            cp16z(slot<F>(S, ks, 3 + 3 * kT, L.lane), p.d2 + mo, mon);
-        } else {
-            cp16(slot<F>(S, ks, 2 + 3 * kT, L.lane), p.d1 + mo);
-            cp16(slot<F>(S, ks, 3 + 3 * kT, L.lane), p.d2 + mo);
-        }
-    }
-    if (PASS != kBackOnly) {
-        if (CHECK) cptz<E>(slot<F>(S, ks, 1, L.lane), p.e + mo, mon);
-        else cpt<E>(slot<F>(S, ks, 1, L.lane), p.e + mo);
-    }
+    constexpr int R = kTile / P;
+    constexpr unsigned kRayBox = kRB * R * sizeof(double2), kEBox = kRB * R * sizeof(E),
+                       kLaneBox = kRB * kTile * sizeof(V);
+    unsigned bytes = kRayBox;                                      // u
+    if (PASS != kBackOnly) bytes += kEBox + kT * kLaneBox;         // e, q
+    if (PASS != kElimOnly) bytes += 2 * kT * kLaneBox;             // w, g
+    if (PASS == kRefineUp) bytes += 2 * kRayBox;                   // d1, d2
+    const int lo = DOWN ? b * kRB : L.span - kRB - b * kRB;
+    const int lm = PASS == kRefineUp ? lo + 1 : (DOWN ? lo - 2 : lo + 2);
+    unsigned long long* bar = &ring_ctl<F>(S)->bar[slot];
+    unsigned char* blk = ring_block<F>(S, slot);
+    const SumMaps& m = a.maps;
+    mbar_expect(bar, bytes);
+    tma_2d(blk + Lay::u, &m.ray[kMapU][P - 1], 0, L.yray + lo, bar);
+    if (PASS != kBackOnly) tma_2d(blk + Lay::e, &m.ray[DOWN ? kMapED : kMapEU][P - 1], 0, L.yray + lm, bar);
 #pragma unroll
     for (int t = 0; t < kT; ++t) {
+        const int yl = L.ylane + t * L.rows;
+        unsigned char* tb = blk + Lay::w0 + 3 * t * Lay::kLane;
         if (PASS != kElimOnly) {
-            if (CHECK) {
-                cptz<V>(slot<F>(S, ks, 2 + 3 * t, L.lane), p.w[t] + ro, on);
-                cptz<V>(slot<F>(S, ks, 3 + 3 * t, L.lane), p.g[t] + ro, on);
-            } else {
-                cpt<V>(slot<F>(S, ks, 2 + 3 * t, L.lane), p.w[t] + ro);
-                cpt<V>(slot<F>(S, ks, 3 + 3 * t, L.lane), p.g[t] + ro);
-            }
+            tma_2d(tb, &m.lane[DOWN ? kMapWU : kMapWD], 0, yl + lo, bar);
+            tma_2d(tb + Lay::kLane, &m.lane[kMapG], 0, yl + lo, bar);
         }
-        if (PASS != kBackOnly) {
-            if (CHECK) cptz<V>(slot<F>(S, ks, 4 + 3 * t, L.lane), p.q[t] + mo, mon);
-            else cpt<V>(slot<F>(S, ks, 4 + 3 * t, L.lane), p.q[t] + mo);
-        }
+        if (PASS != kBackOnly) tma_2d(tb + 2 * Lay::kLane, &m.lane[DOWN ? kMapQD : kMapQU], 0, yl + lm, bar);
     }
-    cp_commit();
+    if constexpr (PASS == kRefineUp) {
+        tma_2d(blk + Lay::d1, &m.ray[kMapED][P - 1], 0, L.yray + lm, bar);
+        tma_2d(blk + Lay::d2, &m.ray[kMapE2][P - 1], 0, L.yray + lm, bar);
+    }
 }
 
 // Thomas factorisation of (M + pole_t D) for this lane's terms, one direction.
@@ -335,11 +354,11 @@ __device__ void sum_factor(const SumArgs& a, const Lane& L, SumSmem& S, const Op
         cp_wait<kSR - 1>();
         EnvRow er;
         {
-            const float* f = sfl<F>(S, slot, L.lane);
+            const float* f = sfl(S, slot, L.lane);
             er.f1 = f[0];
             er.f2 = f[1];
             er.f3 = f[2];
-            er.k = *sks<F>(S, slot, L.lane);
+            er.k = *sks(S, slot, L.lane);
         }
         sum_issue<F, DOWN>(a, L, S, slot, row_of<DOWN>(L, k + kSR), nz);
         if (r < 0 || r > nz + 1) continue;
@@ -428,21 +447,29 @@ struct RowF {
     double2 d1, d2;  // refined form, pass kRefineUp: the residual row's d1 and d2
 };
 
-template <int F>
-__device__ __forceinline__ void load_row(const SumSmem& S, int ks, int lane, RowF<F>& f) {
+// Row j (memory order) of a ring block, for this lane: the ray's u and e (d1,
+// d2), the lane's w, g, q of each term slot - only what the pass uses.
+template <int F, int P, int PASS>
+__device__ __forceinline__ void load_row(const unsigned char* blk, int j, const Lane& L, RowF<F>& f) {
+    using Lay = RingLayout<F>;
     using V = typename Form<F>::V;
     using E = typename Form<F>::E;
-    f.u = *slot<F>(S, ks, 0, lane);
-    f.e = *reinterpret_cast<const E*>(slot<F>(S, ks, 1, lane));
+    constexpr int R = kTile / P;
+    const int ri = j * R + L.slot, li = j * kTile + L.lane;
+    f.u = reinterpret_cast<const double2*>(blk + Lay::u)[ri];
+    if (PASS != kBackOnly) f.e = reinterpret_cast<const E*>(blk + Lay::e)[ri];
 #pragma unroll
     for (int t = 0; t < kT; ++t) {
-        f.w[t] = *reinterpret_cast<const V*>(slot<F>(S, ks, 2 + 3 * t, lane));
-        f.g[t] = *reinterpret_cast<const V*>(slot<F>(S, ks, 3 + 3 * t, lane));
-        f.q[t] = *reinterpret_cast<const V*>(slot<F>(S, ks, 4 + 3 * t, lane));
+        const unsigned char* tb = blk + Lay::w0 + 3 * t * Lay::kLane;
+        if (PASS != kElimOnly) {
+            f.w[t] = reinterpret_cast<const V*>(tb)[li];
+            f.g[t] = reinterpret_cast<const V*>(tb + Lay::kLane)[li];
+        }
+        if (PASS != kBackOnly) f.q[t] = reinterpret_cast<const V*>(tb + 2 * Lay::kLane)[li];
     }
-    if constexpr (F == kRefined) {
-        f.d1 = *slot<F>(S, ks, 2 + 3 * kT, lane);
-        f.d2 = *slot<F>(S, ks, 3 + 3 * kT, lane);
+    if constexpr (PASS == kRefineUp) {
+        f.d1 = reinterpret_cast<const double2*>(blk + Lay::d1)[ri];
+        f.d2 = reinterpret_cast<const double2*>(blk + Lay::d2)[ri];
     }
 }
 
@@ -512,12 +539,13 @@ __device__ __forceinline__ void solve_row(const PassPtrs<F>& p, const Lane& L, c
         const bool first = CHECK ? (DOWN ? (r == 1) : (r == nz)) : false;
         H v;
         if constexpr (F == kFast) {
-            const float2 uf = dn2<float2>(f.u);  // zero-filled except in lane 0
+            const float2 uf = dn2<float2>(f.u);
             v.x = fmaf(o.cinff.x, uf.x, -o.cinff.y * uf.y);
             v.y = fmaf(o.cinff.x, uf.y, o.cinff.y * uf.x);
         } else {
-            v = cmul(o.cinf, f.u);  // f.u is zero-filled except in lane 0
+            v = cmul(o.cinf, f.u);
         }
+        v = hsel(L.k == 0, v, hzero);  // c_inf u_old is lane 0's share
 #pragma unroll
         for (int t = 0; t < kT; ++t) {
             V x;
@@ -660,19 +688,35 @@ __device__ __forceinline__ void refine_row(const PassPtrs<F>& p, const Lane& L, 
     }
 }
 
-// Iterations [k0, k1) of a solve pass, kU rows each.
+// Position of a solve pass in the CTA's ring.
+struct RingPos {
+    unsigned seq0;  // ring sequence number of the pass's block 0
+    int nblk;       // blocks of the pass
+    bool dead;      // a wait gave up (this pass or earlier): wait no more
+};
+
+// Iterations [k0, k1) of a solve pass, kU rows each.  At the first iteration
+// of a block every lane waits for the block's copies; once every lane has
+// read the block's last rows, lane 0 refills the slot with block b + kNB.
 template <int F, int P, int PASS, bool DOWN, bool CHECK>
-__device__ __forceinline__ void solve_iters(const PassPtrs<F>& p, const Lane& L, SumSmem& S, const Ops& o, int k0,
-                                            int k1, SolveState<F>& st) {
+__device__ __forceinline__ void solve_iters(const SumArgs& a, const PassPtrs<F>& p, const Lane& L, SumSmem& S,
+                                            const Ops& o, int k0, int k1, SolveState<F>& st, RingPos& rp) {
+    constexpr int NB = RingLayout<F>::kNB;
 #pragma unroll 1
     for (int k = k0; k < k1; k += kU) {
-        cp_wait<kSR - kU>();
+        const int b = k / kRB, jk = k % kRB;
+        const unsigned q = rp.seq0 + (unsigned)b;
+        const unsigned slot = q % NB;
+        const unsigned char* blk = ring_block<F>(S, slot);
+        if (jk == 0 && !rp.dead)
+            rp.dead = !mbar_wait_bounded(&ring_ctl<F>(S)->bar[slot], (q / NB) & 1u, kRingWaitLimit);
         RowF<F> f[kU];
 #pragma unroll
-        for (int j = 0; j < kU; ++j) load_row<F>(S, (k + j) & (kSR - 1), L.lane, f[j]);
-#pragma unroll
-        for (int j = 0; j < kU; ++j)
-            solve_issue<F, PASS, DOWN, CHECK>(p, L, S, (k + j) & (kSR - 1), row_of<DOWN>(L, k + j + kSR), o.nz);
+        for (int j = 0; j < kU; ++j) load_row<F, P, PASS>(blk, DOWN ? jk + j : kRB - 1 - jk - j, L, f[j]);
+        if (jk + kU == kRB) {
+            __syncwarp(L.wmask);
+            if (L.lane == 0 && b + NB < rp.nblk) ring_issue<F, P, PASS, DOWN>(a, L, S, b + NB, slot);
+        }
 #pragma unroll
         for (int j = 0; j < kU; ++j) {
             if constexpr (PASS == kRefineUp) refine_row<F, P, CHECK>(p, L, o, f[j], row_of<DOWN>(L, k + j), st);
@@ -681,21 +725,70 @@ __device__ __forceinline__ void solve_iters(const PassPtrs<F>& p, const Lane& L,
     }
 }
 
+// Whole blocks [b0, b1) of a solve pass whose rows need no checks: one wait
+// per block, then its kRB rows, kU per step, with the refill after the last
+// rows are read.
+template <int F, int P, int PASS, bool DOWN>
+__device__ __forceinline__ void solve_blocks(const SumArgs& a, const PassPtrs<F>& p, const Lane& L, SumSmem& S,
+                                             const Ops& o, int b0, int b1, SolveState<F>& st, RingPos& rp) {
+    constexpr int NB = RingLayout<F>::kNB;
+    unsigned q = rp.seq0 + (unsigned)b0;
+    unsigned slot = q % NB, parity = (q / NB) & 1u;
+    unsigned long long* bars = ring_ctl<F>(S)->bar;
+#pragma unroll 1
+    for (int b = b0; b < b1; ++b) {
+        const unsigned char* blk = ring_block<F>(S, slot);
+        if (!rp.dead) rp.dead = !mbar_wait_bounded(&bars[slot], parity, kRingWaitLimit);
+#pragma unroll
+        for (int jj = 0; jj < kRB; jj += kU) {
+            RowF<F> f[kU];
+#pragma unroll
+            for (int j = 0; j < kU; ++j) load_row<F, P, PASS>(blk, DOWN ? jj + j : kRB - 1 - jj - j, L, f[j]);
+            if (jj + kU == kRB) {
+                __syncwarp(L.wmask);
+                if (L.lane == 0 && b + NB < rp.nblk) ring_issue<F, P, PASS, DOWN>(a, L, S, b + NB, slot);
+            }
+#pragma unroll
+            for (int j = 0; j < kU; ++j) {
+                const int r = row_of<DOWN>(L, b * kRB + jj + j);
+                if constexpr (PASS == kRefineUp) refine_row<F, P, false>(p, L, o, f[j], r, st);
+                else solve_row<F, P, PASS, DOWN, false>(p, L, o, f[j], r, st);
+            }
+        }
+        if (++slot == NB) {
+            slot = 0;
+            parity ^= 1u;
+        }
+    }
+}
+
 // One solve pass.  kElimOnly: eliminate from the stored field u.  kFusedP:
 // back-substitute the pending solves, combine the terms into u_new (stored
 // by lane 0 of the ray), eliminate the next solves.  kBackOnly:
 // back-substitute and combine only.  Rows are streamed in the pass
-// direction, kU per iteration.
+// direction, kU per iteration, in ring blocks of kRB rows.
 template <int F, int P, int PASS, bool DOWN>
 __device__ void sum_pass(const SumArgs& a, const Lane& L, SumSmem& S, const Ops& o) {
     using V = typename Form<F>::V;
     using H = typename Form<F>::H;
     const int nz = o.nz;
     const PassPtrs<F> p = pass_ptrs<F, DOWN>(a, L);
+    RingCtl* ctl = ring_ctl<F>(S);
+    // The field, the workspace and the factors were last written by generic
+    // stores (the previous pass or factorisation) and the factor ring by
+    // cp.async; the bulk copies write and read through the async proxy.
     __threadfence_block();
+    fence_proxy_async();
     __syncwarp(L.wmask);
+    RingPos rp;
+    rp.seq0 = ctl->seq;
+    rp.dead = ctl->dead != 0;
+    rp.nblk = (L.span + kRB - 1) / kRB;
+    if (L.lane == 0) {
+        constexpr int NB = RingLayout<F>::kNB;
 #pragma unroll 1
-    for (int k = 0; k < kSR; ++k) solve_issue<F, PASS, DOWN, true>(p, L, S, k, row_of<DOWN>(L, k), nz);
+        for (int b = 0; b < NB && b < rp.nblk; ++b) ring_issue<F, P, PASS, DOWN>(a, L, S, b, (rp.seq0 + b) % NB);
+    }
     SolveState<F> st;
     st.h1.x = st.h1.y = 0;
     st.h2 = st.h3 = st.h1;
@@ -705,17 +798,17 @@ __device__ void sum_pass(const SumArgs& a, const Lane& L, SumSmem& S, const Ops&
         st.xq[t].x = st.xq[t].y = 0;
         st.gp[t].x = st.gp[t].y = 0;
     }
-    // Iterations whose rows r (and elimination rows, and the rows they
-    // prefetch) are interior rows of every ray of the warp, and past every
-    // first back-substitution row, run unchecked:
-    //   DOWN: 3 <= r and r + kSR <= nzmin + 1;   UP: kSR <= r <= nzmin - 2.
-    const int lb = DOWN ? 3 : L.span + 1 - L.nzmin;
-    const int ub = DOWN ? L.nzmin + 2 - kSR - kU : L.span - kU - kSR;  // last steady start
-    const int k_lo = min(L.span, (max(lb, 0) + kU - 1) / kU * kU);
-    const int k_hi = ub < k_lo ? k_lo : min(L.span, (ub / kU) * kU + kU);
-    solve_iters<F, P, PASS, DOWN, true>(p, L, S, o, 0, k_lo, st);
-    solve_iters<F, P, PASS, DOWN, false>(p, L, S, o, k_lo, k_hi, st);
-    solve_iters<F, P, PASS, DOWN, true>(p, L, S, o, k_hi, L.span, st);
+    // Iterations whose rows r (and elimination rows) are interior rows of
+    // every ray of the warp, and past every first back-substitution row, run
+    // unchecked, in whole blocks:  DOWN: 3 <= r <= nzmin;  UP: 1 <= r <= nzmin - 2.
+    const int lb = DOWN ? 3 : L.span + 1 - L.nzmin;            // first steady iteration
+    const int ub = DOWN ? L.nzmin + 1 - kU : L.span - kU - 1;  // last steady start
+    const int b_lo = (max(lb, 0) + kRB - 1) / kRB;
+    const int b_hi = max(b_lo, (ub + kU) / kRB);  // blocks [b_lo, b_hi) lie in [lb, ub + kU)
+    const int k_lo = min(L.span, b_lo * kRB), k_hi = min(L.span, b_hi * kRB);
+    solve_iters<F, P, PASS, DOWN, true>(a, p, L, S, o, 0, k_lo, st, rp);
+    solve_blocks<F, P, PASS, DOWN>(a, p, L, S, o, k_lo / kRB, k_hi / kRB, st, rp);
+    solve_iters<F, P, PASS, DOWN, true>(a, p, L, S, o, k_hi, L.span, st, rp);
     // The last row to eliminate (m = nz DOWN, m = 1 UP) would need stream row
     // nz+2 / -1; its window (u_{m-1}, u_m, u_{m+1}) is already in the history.
     // (The residual pass eliminates one row behind the stream: row 1 came with
@@ -730,7 +823,12 @@ __device__ void sum_pass(const SumArgs& a, const Lane& L, SumSmem& S, const Ops&
         for (int t = 0; t < kT; ++t) p.g[t][m * kTile] = st.gp[t];
     }
     (void)sizeof(H);
-    cp_wait<0>();
+    // every block of the pass has been waited for: the ring is idle
+    const bool dead = __any_sync(L.wmask, rp.dead);
+    if (L.lane == 0) {
+        ctl->seq = rp.seq0 + (unsigned)rp.nblk;
+        ctl->dead = dead ? 1u : 0u;
+    }
     __threadfence_block();
     __syncwarp(L.wmask);
 }
@@ -824,6 +922,9 @@ __device__ __forceinline__ void march_tile(const SumArgs& a, SumSmem& S, int t) 
     const RayDev ry = a.rays[rid];
     L.rcol = ry.col;
     L.lcol = a.tile_loff[t] + L.lane;
+    L.slot = (int)(ry.col % kTile);
+    L.yray = (int)(ry.col / kTile);
+    L.ylane = (int)(a.tile_loff[t] / kTile);
     // the warp marches in lockstep: every pass covers the deepest ray's rows,
     // the step loop the longest ray's steps
     L.rows = (int)__reduce_max_sync(L.wmask, (unsigned)(ry.nz + 2));
@@ -1005,17 +1106,32 @@ __device__ __forceinline__ void march_tile(const SumArgs& a, SumSmem& S, int t) 
         r = r_out;
     }
     CR_BACK_ONLY();
+    if (ring_ctl<F>(S)->dead) flag |= 2;  // a wait on the ring gave up: the outputs are not to be trusted
     if (L.k == 0) a.flags[rid] = flag;
 }
 
 #undef CR_FINISH_PENDING
 #undef CR_BACK_ONLY
 
+// The ring's mbarriers, initialised by lane 0 before any copy is issued.
+template <int F>
+__device__ __forceinline__ void ring_init(SumSmem& S) {
+    RingCtl* c = ring_ctl<F>(S);
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < RingLayout<F>::kNB; ++i) mbar_init1(&c->bar[i]);
+        c->seq = 0;
+        c->dead = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+}
+
 // One tile per CTA (one launch per lanes-per-ray value P).
 template <int F, int P>
-__global__ void __launch_bounds__(kTile) march_sum_kernel(SumArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void __launch_bounds__(kTile) march_sum_kernel(const __grid_constant__ SumArgs a) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     SumSmem& S = *reinterpret_cast<SumSmem*>(smem_raw);
+    ring_init<F>(S);
     march_tile<F, P>(a, S, a.tile_begin + blockIdx.x);
 }
 
@@ -1032,9 +1148,10 @@ __device__ __forceinline__ void march_tile_p(const SumArgs& a, SumSmem& S, int t
 // over a.queue, the tiles in longest-march-first order - until the queue is
 // empty, whatever its lanes per ray.  Taking a ticket never waits.
 template <int F>
-__global__ void __launch_bounds__(kTile) march_sum_queue_kernel(SumArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__global__ void __launch_bounds__(kTile) march_sum_queue_kernel(const __grid_constant__ SumArgs a) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
     SumSmem& S = *reinterpret_cast<SumSmem*>(smem_raw);
+    ring_init<F>(S);
     for (;;) {
         int k = 0;
         if (threadIdx.x == 0) k = atomicAdd(a.ticket, 1);

@@ -27,6 +27,7 @@
 #include <cstdlib>
 
 #include "../../include/cupyram_b200_mlp.h"
+#include "tensor_map.h"
 
 namespace {
 
@@ -770,24 +771,8 @@ __global__ void __launch_bounds__(kPThreads, 1) gemm_tn_persistent(const __grid_
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * UBN));
 }
 
-// cuTensorMapEncodeTiled, reached through the runtime's driver entry point
-// (the library links no driver library).
-using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-EncodeTiledFn encode_tiled() {
-    static EncodeTiledFn fn = nullptr;
-    static bool tried = false;
-    if (!tried) {
-        tried = true;
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = (EncodeTiledFn)p;
-    }
-    return fn;
-}
+using crk::encode_tiled;
+using crk::EncodeTiledFn;
 
 // Tensor map of a rows x K bf16 operand (row stride ld elements) in boxes of
 // `box_rows` rows x 64 elements, 128-byte swizzle: the layout the MMAs read.

@@ -36,8 +36,8 @@ enum cr_status {
     CR_EINVAL = 1,    /* invalid argument or inconsistent batch description */
     CR_ECUDA = 2,     /* CUDA runtime error (text in cr_last_error)          */
     CR_EPADE = 3,     /* Pade root finding did not converge                   */
-    CR_ETIMEOUT = 4,  /* a device-side iteration cap was hit (reserved: the
-                         march kernels have no waits of their own)            */
+    CR_ETIMEOUT = 4,  /* a device-side wait gave up: the batched march's
+                         waits for its bulk copies are bounded (flag bit 1)  */
     CR_ENAN = 5,      /* a ray produced a non-finite field (see cr_ray_flags) */
     CR_ENOMEM = 6,    /* device or host allocation failed                     */
     CR_ESTATE = 7     /* call made in the wrong order (e.g. march before upload) */
@@ -226,7 +226,8 @@ int cr_cell_tl(cr_engine* e, int sz, int sr, int ncz, int ncr, float* tl_cells);
  * 1 self-starter ip=2, 2 march, 3 march after rs.  n terms (<= CR_MAX_NP). */
 int cr_set_pade(cr_engine* e, int ray, int which, int n, const double* pd1, const double* pd2);
 
-/* Per-ray status flags of the last march (bit 0: non-finite field). */
+/* Per-ray status flags of the last march (bit 0: non-finite field; bit 1: a
+   bounded wait for the batched march's bulk copies gave up, CR_ETIMEOUT). */
 int cr_ray_flags(cr_engine* e, int32_t* flags, int n);
 
 int cr_get_stats(const cr_engine* e, cr_stats* st);
