@@ -1586,6 +1586,10 @@ int cr_create(const cr_batch* b, cr_engine** out) {
     }
     if (ce == cudaSuccess)
         ce = cudaFuncSetAttribute(march_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kRingBytes);
+    // the batched march's kernels are loaded now, while the device is idle,
+    // not at their first launch beside running column clusters
+    if (ce == cudaSuccess && e->sum_mode && e->n_tiles > 0)
+        ce = crk::prepare_march_sum(e->tile_G.data(), e->n_tiles, e->precision);
     if (ce != cudaSuccess) {
         set_global_error("cr_create: %s", cudaGetErrorString(ce));
         const int code = ce == cudaErrorMemoryAllocation ? CR_ENOMEM : CR_ECUDA;
@@ -1781,6 +1785,7 @@ int cr_march(cr_engine* e) {
             if (ce == cudaSuccess && e->n_tiles > 0) ce = cudaMemsetAsync(e->d_ticket, 0, sizeof(int), e->stream);
             if (ce == cudaSuccess && e->n_tiles > 0) {
                 sa.max_ctas = 0;
+                sa.min_p = *std::min_element(e->tile_G.begin(), e->tile_G.end());
                 ce = crk::launch_march_sum_queue(sa, e->n_tiles, e->precision, e->stream, &ctas);
                 nb = 1;
             }

@@ -55,21 +55,36 @@ bool encode_sum_maps(SumArgs& a, int form, long long ray_rows, long long lane_ro
     return ok;
 }
 
-cudaError_t sum_launch_plain(const SumArgs& a, int p, int count, cudaStream_t st);
-cudaError_t sum_launch_chosen(const SumArgs& a, int p, int count, cudaStream_t st);
-cudaError_t sum_launch_fast(const SumArgs& a, int p, int count, cudaStream_t st);
-cudaError_t sum_queue_plain(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas);
-cudaError_t sum_queue_chosen(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas);
-cudaError_t sum_queue_fast(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas);
-cudaError_t sum_launch_refined(const SumArgs& a, int p, int count, cudaStream_t st);
-cudaError_t sum_queue_refined(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas);
+cudaError_t sum_launch_plain(const SumArgs& a, int p, int count, cudaStream_t st, bool launch);
+cudaError_t sum_launch_chosen(const SumArgs& a, int p, int count, cudaStream_t st, bool launch);
+cudaError_t sum_launch_fast(const SumArgs& a, int p, int count, cudaStream_t st, bool launch);
+cudaError_t sum_launch_refined(const SumArgs& a, int p, int count, cudaStream_t st, bool launch);
+cudaError_t sum_queue_plain(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas, bool launch);
+cudaError_t sum_queue_chosen(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas, bool launch);
+cudaError_t sum_queue_fast(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas, bool launch);
+cudaError_t sum_queue_refined(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas, bool launch);
+
+namespace {
+
+cudaError_t queue_form(const SumArgs& a, int n_tiles, int form, cudaStream_t st, int* ctas, bool launch) {
+    return form == CR_C64_REFINED ? sum_queue_refined(a, n_tiles, st, ctas, launch)
+           : form == CR_CHOSEN_C64 ? sum_queue_fast(a, n_tiles, st, ctas, launch)
+           : form == CR_CHOSEN_C64R ? sum_queue_chosen(a, n_tiles, st, ctas, launch)
+                                    : sum_queue_plain(a, n_tiles, st, ctas, launch);
+}
+
+cudaError_t launch_form(const SumArgs& a, int p, int count, int form, cudaStream_t st, bool launch) {
+    return form == CR_C64_REFINED ? sum_launch_refined(a, p, count, st, launch)
+           : form == CR_CHOSEN_C64 ? sum_launch_fast(a, p, count, st, launch)
+           : form == CR_CHOSEN_C64R ? sum_launch_chosen(a, p, count, st, launch)
+                                    : sum_launch_plain(a, p, count, st, launch);
+}
+
+}  // namespace
 
 cudaError_t launch_march_sum_queue(const SumArgs& a, int n_tiles, int form, cudaStream_t st, int* ctas) {
     if (n_tiles <= 0) return cudaSuccess;
-    return form == CR_C64_REFINED ? sum_queue_refined(a, n_tiles, st, ctas)
-           : form == CR_CHOSEN_C64 ? sum_queue_fast(a, n_tiles, st, ctas)
-           : form == CR_CHOSEN_C64R ? sum_queue_chosen(a, n_tiles, st, ctas)
-                                    : sum_queue_plain(a, n_tiles, st, ctas);
+    return queue_form(a, n_tiles, form, st, ctas, true);
 }
 
 cudaError_t launch_march_sum(const SumArgs& a0, const int* tile_P, int n_tiles, int form,
@@ -83,15 +98,27 @@ cudaError_t launch_march_sum(const SumArgs& a0, const int* tile_P, int n_tiles, 
         SumArgs a = a0;
         a.tile_begin = begin;
         const cudaStream_t st = streams[*launches % n_streams];
-        const cudaError_t ce = form == CR_C64_REFINED ? sum_launch_refined(a, tile_P[begin], end - begin, st)
-                               : form == CR_CHOSEN_C64 ? sum_launch_fast(a, tile_P[begin], end - begin, st)
-                               : form == CR_CHOSEN_C64R ? sum_launch_chosen(a, tile_P[begin], end - begin, st)
-                                                        : sum_launch_plain(a, tile_P[begin], end - begin, st);
+        const cudaError_t ce = launch_form(a, tile_P[begin], end - begin, form, st, true);
         if (ce != cudaSuccess) return ce;
         ++*launches;
         begin = end;
     }
     return cudaSuccess;
+}
+
+cudaError_t prepare_march_sum(const int* tile_P, int n_tiles, int form) {
+    SumArgs a{};
+    a.min_p = kMaxP;
+    bool seen[kMaxP + 1] = {};
+    for (int t = 0; t < n_tiles; ++t)
+        if (tile_P[t] >= 1 && tile_P[t] <= kMaxP) {
+            seen[tile_P[t]] = true;
+            a.min_p = tile_P[t] < a.min_p ? tile_P[t] : a.min_p;
+        }
+    cudaError_t ce = n_tiles > 0 ? queue_form(a, n_tiles, form, 0, nullptr, false) : cudaSuccess;
+    for (int p = 1; p <= kMaxP && ce == cudaSuccess; ++p)
+        if (seen[p]) ce = launch_form(a, p, 0, form, 0, false);
+    return ce;
 }
 
 }  // namespace crk

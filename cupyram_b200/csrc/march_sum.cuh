@@ -86,6 +86,7 @@ struct SumArgs {
     const int* queue;
     int n_queue;
     int max_ctas;  // persistent launch: CTAs = every resident slot (0), or this many
+    int min_p;     // persistent launch: the smallest lanes-per-ray value among the tiles
     SumMaps maps;  // the kernels take SumArgs as a __grid_constant__ parameter
 };
 
@@ -113,5 +114,10 @@ cudaError_t launch_march_sum_queue(const SumArgs& a, int n_tiles, int form, cuda
 
 cudaError_t launch_march_sum(const SumArgs& a, const int* tile_P, int n_tiles, int form,
                              const cudaStream_t* streams, int n_streams, int* launches);
+
+// Loads the kernels (and sets the shared-memory limits) that the two
+// launchers above use for these tiles, so that no kernel is loaded at its
+// first launch while other streams' kernels run.
+cudaError_t prepare_march_sum(const int* tile_P, int n_tiles, int form);
 
 }  // namespace crk

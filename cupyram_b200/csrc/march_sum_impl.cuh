@@ -113,20 +113,24 @@ struct Form<kFast> {
 };
 
 // Shared memory of a CTA (one warp), from its base:
-//   * the solve passes' ring: kNB blocks (ring_blocks of the form), each holding kRB rows of every field
-//     a solve pass streams, in 128-byte aligned regions (RingLayout<F>): the
-//     ray fields u, e (and d1, d2) as [kRB][floor(32 / P)] (the tile's rays),
-//     the lane fields w, g, q of each term slot as [kRB][32];
-//   * over the same bytes, the factor passes' cp.async ring, [kSR][2][32]
+//   * RingCtl (kCtlBytes): the ring's mbarriers and position, which persist
+//     across the tiles a CTA marches;
+//   * the solve passes' ring: kNB blocks (ring_blocks of the form), each
+//     holding kRB rows of every field a solve pass streams, in 128-byte
+//     aligned regions (RingLayout<F, P>): the ray fields u, e (and d1, d2) as
+//     [kRB][floor(32 / P)] (the tile's rays), the lane fields w, g, q of each
+//     term slot as [kRB][32];
+//   * over the ring's bytes, the factor passes' cp.async ring, [kSR][2][32]
 //     16-byte slots (f1..f3 and ksq of each lane's ray row): a factor pass
-//     runs only between solve passes, whose copies have all landed;
-//   * after both, RingCtl: the ring's mbarriers and position.
-template <int F>
+//     runs only between solve passes, whose copies have all landed.
+__host__ __device__ constexpr int up128(int n) { return (n + 127) / 128 * 128; }
+template <int F, int P>
 struct RingLayout {
     using V = typename Form<F>::V;
     using E = typename Form<F>::E;
-    static constexpr int kRay = kRB * kTile * (int)sizeof(double2);  // u, d1, d2 (room for 32 rays)
-    static constexpr int kE = kRB * kTile * (int)sizeof(E);
+    static constexpr int R = kTile / P;  // rays of the tile
+    static constexpr int kRay = up128(kRB * R * (int)sizeof(double2));  // u, d1, d2
+    static constexpr int kE = up128(kRB * R * (int)sizeof(E));
     static constexpr int kLane = kRB * kTile * (int)sizeof(V);
     static constexpr int u = 0;
     static constexpr int e = u + kRay;
@@ -135,33 +139,29 @@ struct RingLayout {
     static constexpr int d2 = d1 + kRay;
     static constexpr int block = F == kRefined ? d2 + kRay : d1;
     static constexpr int kNB = ring_blocks(F);
-    static_assert(kE % 128 == 0 && kLane % 128 == 0 && kRay % 128 == 0, "regions must stay 128-byte aligned");
+    static_assert(kLane % 128 == 0, "regions must stay 128-byte aligned");
 };
 struct RingCtl {
     unsigned long long bar[kNBMax];  // one mbarrier per ring block (arrival count 1 + the copies' bytes)
     unsigned seq;                    // ring blocks this CTA has consumed: slot seq % kNB, phase (seq / kNB) & 1
-    unsigned dead;                // a wait gave up: later waits are skipped and the CTA's rays are flagged
+    unsigned dead;                   // a wait gave up: later waits are skipped and the CTA's rays are flagged
 };
+constexpr int kCtlBytes = 128;
+static_assert(sizeof(RingCtl) <= kCtlBytes, "RingCtl must fit its slot");
 constexpr int kFactorRing = kSR * 2 * kTile * (int)sizeof(double2);
-template <int F>
-__host__ __device__ constexpr size_t ring_bytes() {
-    using Lay = RingLayout<F>;
-    return (size_t)(Lay::kNB * Lay::block > kFactorRing ? Lay::kNB * Lay::block : kFactorRing);
-}
-template <int F>
+// dynamic shared memory of a CTA marching tiles of P lanes per ray
+template <int F, int P>
 __host__ __device__ constexpr size_t smem_of() {
-    return ring_bytes<F>() + sizeof(RingCtl);
+    using Lay = RingLayout<F, P>;
+    return (size_t)kCtlBytes + (size_t)(Lay::kNB * Lay::block > kFactorRing ? Lay::kNB * Lay::block : kFactorRing);
 }
 struct SumSmem {
     double2 d[1];
 };
-template <int F>
-__device__ __forceinline__ RingCtl* ring_ctl(SumSmem& S) {
-    return reinterpret_cast<RingCtl*>(reinterpret_cast<unsigned char*>(&S) + ring_bytes<F>());
-}
-template <int F>
+__device__ __forceinline__ RingCtl* ring_ctl(SumSmem& S) { return reinterpret_cast<RingCtl*>(&S); }
+template <int F, int P>
 __device__ __forceinline__ unsigned char* ring_block(SumSmem& S, unsigned slot) {
-    return reinterpret_cast<unsigned char*>(&S) + slot * (unsigned)RingLayout<F>::block;
+    return reinterpret_cast<unsigned char*>(&S) + kCtlBytes + slot * (unsigned)RingLayout<F, P>::block;
 }
 
 __device__ __forceinline__ double2 up2(double2 v) { return v; }
@@ -224,10 +224,12 @@ __device__ __forceinline__ typename Prec<R>::V* facw(double2* p) {
 }
 
 // factor-pass ring slots of prefetch row k: f1..f3 and ksq of the lane's ray row
-__device__ __forceinline__ float* sfl(SumSmem& S, int k, int lane) { return (float*)&S.d[(k * 2) * kTile + lane]; }
-__device__ __forceinline__ float2* sks(SumSmem& S, int k, int lane) {
-    return (float2*)&S.d[(k * 2 + 1) * kTile + lane];
+__device__ __forceinline__ double2* factor_slot(SumSmem& S, int k, int field, int lane) {
+    return reinterpret_cast<double2*>(reinterpret_cast<unsigned char*>(&S) + kCtlBytes) + (k * 2 + field) * kTile +
+           lane;
 }
+__device__ __forceinline__ float* sfl(SumSmem& S, int k, int lane) { return (float*)factor_slot(S, k, 0, lane); }
+__device__ __forceinline__ float2* sks(SumSmem& S, int k, int lane) { return (float2*)factor_slot(S, k, 1, lane); }
 
 // Stream row of iteration k: the same for every lane of the warp.
 template <bool DOWN>
@@ -293,7 +295,7 @@ __device__ __forceinline__ PassPtrs<F> pass_ptrs(const SumArgs& a, const Lane& L
 // they are never used (the CHECK iterations select them away).
 template <int F, int P, int PASS, bool DOWN>
 __device__ __forceinline__ void ring_issue(const SumArgs& a, const Lane& L, SumSmem& S, int b, unsigned slot) {
-    using Lay = RingLayout<F>;
+    using Lay = RingLayout<F, P>;
     using V = typename Form<F>::V;
     using E = typename Form<F>::E;
     constexpr int R = kTile / P;
@@ -305,8 +307,8 @@ __device__ __forceinline__ void ring_issue(const SumArgs& a, const Lane& L, SumS
     if (PASS == kRefineUp) bytes += 2 * kRayBox;                   // d1, d2
     const int lo = DOWN ? b * kRB : L.span - kRB - b * kRB;
     const int lm = PASS == kRefineUp ? lo + 1 : (DOWN ? lo - 2 : lo + 2);
-    unsigned long long* bar = &ring_ctl<F>(S)->bar[slot];
-    unsigned char* blk = ring_block<F>(S, slot);
+    unsigned long long* bar = &ring_ctl(S)->bar[slot];
+    unsigned char* blk = ring_block<F, P>(S, slot);
     const SumMaps& m = a.maps;
     mbar_expect(bar, bytes);
     tma_2d(blk + Lay::u, &m.ray[kMapU][P - 1], 0, L.yray + lo, bar);
@@ -451,7 +453,7 @@ struct RowF {
 // d2), the lane's w, g, q of each term slot - only what the pass uses.
 template <int F, int P, int PASS>
 __device__ __forceinline__ void load_row(const unsigned char* blk, int j, const Lane& L, RowF<F>& f) {
-    using Lay = RingLayout<F>;
+    using Lay = RingLayout<F, P>;
     using V = typename Form<F>::V;
     using E = typename Form<F>::E;
     constexpr int R = kTile / P;
@@ -701,15 +703,15 @@ struct RingPos {
 template <int F, int P, int PASS, bool DOWN, bool CHECK>
 __device__ __forceinline__ void solve_iters(const SumArgs& a, const PassPtrs<F>& p, const Lane& L, SumSmem& S,
                                             const Ops& o, int k0, int k1, SolveState<F>& st, RingPos& rp) {
-    constexpr int NB = RingLayout<F>::kNB;
+    constexpr int NB = RingLayout<F, P>::kNB;
 #pragma unroll 1
     for (int k = k0; k < k1; k += kU) {
         const int b = k / kRB, jk = k % kRB;
         const unsigned q = rp.seq0 + (unsigned)b;
         const unsigned slot = q % NB;
-        const unsigned char* blk = ring_block<F>(S, slot);
+        const unsigned char* blk = ring_block<F, P>(S, slot);
         if (jk == 0 && !rp.dead)
-            rp.dead = !mbar_wait_bounded(&ring_ctl<F>(S)->bar[slot], (q / NB) & 1u, kRingWaitLimit);
+            rp.dead = !mbar_wait_bounded(&ring_ctl(S)->bar[slot], (q / NB) & 1u, kRingWaitLimit);
         RowF<F> f[kU];
 #pragma unroll
         for (int j = 0; j < kU; ++j) load_row<F, P, PASS>(blk, DOWN ? jk + j : kRB - 1 - jk - j, L, f[j]);
@@ -731,13 +733,13 @@ __device__ __forceinline__ void solve_iters(const SumArgs& a, const PassPtrs<F>&
 template <int F, int P, int PASS, bool DOWN>
 __device__ __forceinline__ void solve_blocks(const SumArgs& a, const PassPtrs<F>& p, const Lane& L, SumSmem& S,
                                              const Ops& o, int b0, int b1, SolveState<F>& st, RingPos& rp) {
-    constexpr int NB = RingLayout<F>::kNB;
+    constexpr int NB = RingLayout<F, P>::kNB;
     unsigned q = rp.seq0 + (unsigned)b0;
     unsigned slot = q % NB, parity = (q / NB) & 1u;
-    unsigned long long* bars = ring_ctl<F>(S)->bar;
+    unsigned long long* bars = ring_ctl(S)->bar;
 #pragma unroll 1
     for (int b = b0; b < b1; ++b) {
-        const unsigned char* blk = ring_block<F>(S, slot);
+        const unsigned char* blk = ring_block<F, P>(S, slot);
         if (!rp.dead) rp.dead = !mbar_wait_bounded(&bars[slot], parity, kRingWaitLimit);
 #pragma unroll
         for (int jj = 0; jj < kRB; jj += kU) {
@@ -773,7 +775,7 @@ __device__ void sum_pass(const SumArgs& a, const Lane& L, SumSmem& S, const Ops&
     using H = typename Form<F>::H;
     const int nz = o.nz;
     const PassPtrs<F> p = pass_ptrs<F, DOWN>(a, L);
-    RingCtl* ctl = ring_ctl<F>(S);
+    RingCtl* ctl = ring_ctl(S);
     // The field, the workspace and the factors were last written by generic
     // stores (the previous pass or factorisation) and the factor ring by
     // cp.async; the bulk copies write and read through the async proxy.
@@ -785,7 +787,7 @@ __device__ void sum_pass(const SumArgs& a, const Lane& L, SumSmem& S, const Ops&
     rp.dead = ctl->dead != 0;
     rp.nblk = (L.span + kRB - 1) / kRB;
     if (L.lane == 0) {
-        constexpr int NB = RingLayout<F>::kNB;
+        constexpr int NB = RingLayout<F, P>::kNB;
 #pragma unroll 1
         for (int b = 0; b < NB && b < rp.nblk; ++b) ring_issue<F, P, PASS, DOWN>(a, L, S, b, (rp.seq0 + b) % NB);
     }
@@ -1106,7 +1108,7 @@ __device__ __forceinline__ void march_tile(const SumArgs& a, SumSmem& S, int t) 
         r = r_out;
     }
     CR_BACK_ONLY();
-    if (ring_ctl<F>(S)->dead) flag |= 2;  // a wait on the ring gave up: the outputs are not to be trusted
+    if (ring_ctl(S)->dead) flag |= 2;  // a wait on the ring gave up: the outputs are not to be trusted
     if (L.k == 0) a.flags[rid] = flag;
 }
 
@@ -1116,9 +1118,9 @@ __device__ __forceinline__ void march_tile(const SumArgs& a, SumSmem& S, int t) 
 // The ring's mbarriers, initialised by lane 0 before any copy is issued.
 template <int F>
 __device__ __forceinline__ void ring_init(SumSmem& S) {
-    RingCtl* c = ring_ctl<F>(S);
+    RingCtl* c = ring_ctl(S);
     if (threadIdx.x == 0) {
-        for (int i = 0; i < RingLayout<F>::kNB; ++i) mbar_init1(&c->bar[i]);
+        for (int i = 0; i < ring_blocks(F); ++i) mbar_init1(&c->bar[i]);
         c->seq = 0;
         c->dead = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -1163,31 +1165,47 @@ __global__ void __launch_bounds__(kTile) march_sum_queue_kernel(const __grid_con
     }
 }
 
+// Sets the kernel's shared-memory limit; the first such call also loads the
+// kernel, which is then not loaded at its first launch (a load while other
+// streams' kernels run waits for them).
+template <int F, int P>
+static cudaError_t prepare_one() {
+    return cudaFuncSetAttribute(march_sum_kernel<F, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)smem_of<F, P>());
+}
+
 template <int F, int P>
 static cudaError_t launch_one(const SumArgs& a, int count, cudaStream_t st) {
-    const size_t smem = smem_of<F>();
-    cudaError_t ce = cudaFuncSetAttribute(march_sum_kernel<F, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const cudaError_t ce = prepare_one<F, P>();
     if (ce != cudaSuccess) return ce;
-    march_sum_kernel<F, P><<<count, kTile, smem, st>>>(a);
+    march_sum_kernel<F, P><<<count, kTile, smem_of<F, P>(), st>>>(a);
     return cudaGetLastError();
 }
 
 template <int F, int P = 1>
-static cudaError_t launch_p(const SumArgs& a, int p, int count, cudaStream_t st) {
+static cudaError_t launch_p(const SumArgs& a, int p, int count, cudaStream_t st, bool launch) {
     if constexpr (P > kMaxP) {
         return cudaErrorInvalidValue;
     } else {
-        if (p == P) return launch_one<F, P>(a, count, st);
-        return launch_p<F, P + 1>(a, p, count, st);
+        if (p == P) return launch ? launch_one<F, P>(a, count, st) : prepare_one<F, P>();
+        return launch_p<F, P + 1>(a, p, count, st, launch);
     }
 }
 
+// shared memory of the persistent launch: the largest need of the tiles' P
+// values, i.e. that of the smallest P present
+template <int F, int P = 1>
+static size_t smem_from_p(int p) {
+    if constexpr (P >= kMaxP) return smem_of<F, kMaxP>();
+    else return p <= P ? smem_of<F, P>() : smem_from_p<F, P + 1>(p);
+}
+
 template <int F>
-static cudaError_t launch_queue_f(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas) {
-    const size_t smem = smem_of<F>();
+static cudaError_t launch_queue_f(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas, bool launch) {
+    const size_t smem = smem_from_p<F>(a.min_p);
     cudaError_t ce = cudaFuncSetAttribute(march_sum_queue_kernel<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem);
-    if (ce != cudaSuccess) return ce;
+    if (ce != cudaSuccess || !launch) return ce;
     int dev = 0, sms = 0, per_sm = 0;
     ce = cudaGetDevice(&dev);
     if (ce == cudaSuccess) ce = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

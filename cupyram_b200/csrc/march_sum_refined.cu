@@ -4,12 +4,12 @@
 
 namespace crk {
 
-cudaError_t sum_launch_refined(const SumArgs& a, int p, int count, cudaStream_t st) {
-    return launch_p<kRefined>(a, p, count, st);
+cudaError_t sum_launch_refined(const SumArgs& a, int p, int count, cudaStream_t st, bool launch) {
+    return launch_p<kRefined>(a, p, count, st, launch);
 }
 
-cudaError_t sum_queue_refined(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas) {
-    return launch_queue_f<kRefined>(a, n_tiles, st, ctas);
+cudaError_t sum_queue_refined(const SumArgs& a, int n_tiles, cudaStream_t st, int* ctas, bool launch) {
+    return launch_queue_f<kRefined>(a, n_tiles, st, ctas, launch);
 }
 
 }  // namespace crk
