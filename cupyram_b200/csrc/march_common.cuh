@@ -310,17 +310,33 @@ __device__ __forceinline__ void mbar_expect(unsigned long long* bar, unsigned by
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
 }
-// true once the phase of this parity has completed; false after `limit` polls
+// true once the phase of this parity has completed; false after `limit`
+// polls.  A poll may suspend the thread for up to `suspend_ns` (it resumes
+// when the phase completes), so that a waiting warp does not take issue
+// slots from the SM's other warps.
+#ifndef CR_MBAR_SUSPEND_NS
+#define CR_MBAR_SUSPEND_NS 100
+#endif
 __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, unsigned limit) {
     for (unsigned it = 0; it < limit; ++it) {
         unsigned done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t}"
-            : "=r"(done)
-            : "r"(smem_u32(bar)), "r"(parity)
-            : "memory");
+        if (CR_MBAR_SUSPEND_NS > 0) {
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}"
+                : "=r"(done)
+                : "r"(smem_u32(bar)), "r"(parity), "n"(CR_MBAR_SUSPEND_NS)
+                : "memory");
+        } else {
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}"
+                : "=r"(done)
+                : "r"(smem_u32(bar)), "r"(parity)
+                : "memory");
+        }
         if (done) return true;
     }
     return false;

@@ -66,6 +66,15 @@ constexpr int kU = CR_SUM_ROWS;       // rows per solve-loop iteration
 static_assert((kSR & (kSR - 1)) == 0, "kSR must be a power of two");
 static_assert(kSR % kU == 0, "the prefetch ring must hold whole iterations");
 static_assert(kRB % kU == 0, "a ring block must hold whole iterations");
+#ifndef CR_SUM_BLOCK_UNROLL
+#define CR_SUM_BLOCK_UNROLL (CR_SUM_RB / CR_SUM_ROWS)
+#endif
+constexpr int kBlockUnroll = CR_SUM_BLOCK_UNROLL;  // row steps of a steady block unrolled
+#ifndef CR_SUM_BLOCK_UNROLL_REFINED
+#define CR_SUM_BLOCK_UNROLL_REFINED 2
+#endif
+// the refined form's rows carry more state: a shorter unrolled body keeps it in registers
+constexpr int kBlockUnrollRefined = CR_SUM_BLOCK_UNROLL_REFINED;
 
 enum SumPass { kElimOnly = 0, kFusedP = 1, kBackOnly = 2, kFactor = 3, kRefineUp = 4 };
 
@@ -704,14 +713,19 @@ template <int F, int P, int PASS, bool DOWN, bool CHECK>
 __device__ __forceinline__ void solve_iters(const SumArgs& a, const PassPtrs<F>& p, const Lane& L, SumSmem& S,
                                             const Ops& o, int k0, int k1, SolveState<F>& st, RingPos& rp) {
     constexpr int NB = RingLayout<F, P>::kNB;
+    // ring slot and mbarrier phase of the block holding iteration k, kept
+    // up to date as k crosses block boundaries
+    const unsigned q0 = rp.seq0 + (unsigned)(k0 / kRB);
+    unsigned slot = q0 % NB, parity = (q0 / NB) & 1u;
 #pragma unroll 1
     for (int k = k0; k < k1; k += kU) {
         const int b = k / kRB, jk = k % kRB;
-        const unsigned q = rp.seq0 + (unsigned)b;
-        const unsigned slot = q % NB;
+        if (jk == 0 && k != k0 && ++slot == NB) {
+            slot = 0;
+            parity ^= 1u;
+        }
         const unsigned char* blk = ring_block<F, P>(S, slot);
-        if (jk == 0 && !rp.dead)
-            rp.dead = !mbar_wait_bounded(&ring_ctl(S)->bar[slot], (q / NB) & 1u, kRingWaitLimit);
+        if (jk == 0 && !rp.dead) rp.dead = !mbar_wait_bounded(&ring_ctl(S)->bar[slot], parity, kRingWaitLimit);
         RowF<F> f[kU];
 #pragma unroll
         for (int j = 0; j < kU; ++j) load_row<F, P, PASS>(blk, DOWN ? jk + j : kRB - 1 - jk - j, L, f[j]);
@@ -741,7 +755,8 @@ __device__ __forceinline__ void solve_blocks(const SumArgs& a, const PassPtrs<F>
     for (int b = b0; b < b1; ++b) {
         const unsigned char* blk = ring_block<F, P>(S, slot);
         if (!rp.dead) rp.dead = !mbar_wait_bounded(&bars[slot], parity, kRingWaitLimit);
-#pragma unroll
+        constexpr int kUnroll = F == kRefined ? kBlockUnrollRefined : kBlockUnroll;
+#pragma unroll kUnroll
         for (int jj = 0; jj < kRB; jj += kU) {
             RowF<F> f[kU];
 #pragma unroll
@@ -808,9 +823,13 @@ __device__ void sum_pass(const SumArgs& a, const Lane& L, SumSmem& S, const Ops&
     const int b_lo = (max(lb, 0) + kRB - 1) / kRB;
     const int b_hi = max(b_lo, (ub + kU) / kRB);  // blocks [b_lo, b_hi) lie in [lb, ub + kU)
     const int k_lo = min(L.span, b_lo * kRB), k_hi = min(L.span, b_hi * kRB);
-    solve_iters<F, P, PASS, DOWN, true>(a, p, L, S, o, 0, k_lo, st, rp);
-    solve_blocks<F, P, PASS, DOWN>(a, p, L, S, o, k_lo / kRB, k_hi / kRB, st, rp);
-    solve_iters<F, P, PASS, DOWN, true>(a, p, L, S, o, k_hi, L.span, st, rp);
+    // checked iterations before and after the steady blocks (one copy of
+    // the checked loop)
+#pragma unroll 1
+    for (int seg = 0; seg < 2; ++seg) {
+        solve_iters<F, P, PASS, DOWN, true>(a, p, L, S, o, seg ? k_hi : 0, seg ? L.span : k_lo, st, rp);
+        if (seg == 0) solve_blocks<F, P, PASS, DOWN>(a, p, L, S, o, k_lo / kRB, k_hi / kRB, st, rp);
+    }
     // The last row to eliminate (m = nz DOWN, m = 1 UP) would need stream row
     // nz+2 / -1; its window (u_{m-1}, u_m, u_{m+1}) is already in the history.
     // (The residual pass eliminates one row behind the stream: row 1 came with
