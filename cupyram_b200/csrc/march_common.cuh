@@ -353,6 +353,10 @@ __device__ __forceinline__ void tma_2d(void* dst, const void* map, int x, int y,
 // orders this thread's earlier generic-proxy accesses before later
 // async-proxy (bulk copy) accesses, in global and shared memory
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async;" ::: "memory"); }
+// the same, for shared memory only
+__device__ __forceinline__ void fence_proxy_async_shared() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
 
 struct EnvRow {
     float f1, f2, f3;

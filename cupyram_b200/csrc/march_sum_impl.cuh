@@ -706,9 +706,26 @@ struct RingPos {
     bool dead;      // a wait gave up (this pass or earlier): wait no more
 };
 
+// After the last rows of block b have been used: slot `slot` gets block
+// b + kNB.  The bulk copy writes shared memory directly, not through the
+// load/store pipeline, so it is not ordered behind loads still queued there
+// (other CTAs' shared-memory traffic can hold them back): every lane's loads
+// of the block have been consumed by arithmetic before this point, each
+// lane's proxy fence orders its reads before the async-proxy writes, and the
+// warp synchronises before lane 0 issues.
+template <int F, int P, int PASS, bool DOWN>
+__device__ __forceinline__ void ring_refill(const SumArgs& a, const Lane& L, SumSmem& S, int b, unsigned slot,
+                                            const RingPos& rp) {
+    constexpr int NB = RingLayout<F, P>::kNB;
+    if (b + NB >= rp.nblk) return;  // warp-uniform
+    fence_proxy_async_shared();
+    __syncwarp(L.wmask);
+    if (L.lane == 0) ring_issue<F, P, PASS, DOWN>(a, L, S, b + NB, slot);
+}
+
 // Iterations [k0, k1) of a solve pass, kU rows each.  At the first iteration
 // of a block every lane waits for the block's copies; once every lane has
-// read the block's last rows, lane 0 refills the slot with block b + kNB.
+// used the block's last rows, lane 0 refills the slot with block b + kNB.
 template <int F, int P, int PASS, bool DOWN, bool CHECK>
 __device__ __forceinline__ void solve_iters(const SumArgs& a, const PassPtrs<F>& p, const Lane& L, SumSmem& S,
                                             const Ops& o, int k0, int k1, SolveState<F>& st, RingPos& rp) {
@@ -729,21 +746,18 @@ __device__ __forceinline__ void solve_iters(const SumArgs& a, const PassPtrs<F>&
         RowF<F> f[kU];
 #pragma unroll
         for (int j = 0; j < kU; ++j) load_row<F, P, PASS>(blk, DOWN ? jk + j : kRB - 1 - jk - j, L, f[j]);
-        if (jk + kU == kRB) {
-            __syncwarp(L.wmask);
-            if (L.lane == 0 && b + NB < rp.nblk) ring_issue<F, P, PASS, DOWN>(a, L, S, b + NB, slot);
-        }
 #pragma unroll
         for (int j = 0; j < kU; ++j) {
             if constexpr (PASS == kRefineUp) refine_row<F, P, CHECK>(p, L, o, f[j], row_of<DOWN>(L, k + j), st);
             else solve_row<F, P, PASS, DOWN, CHECK>(p, L, o, f[j], row_of<DOWN>(L, k + j), st);
         }
+        if (jk + kU == kRB) ring_refill<F, P, PASS, DOWN>(a, L, S, b, slot, rp);
     }
 }
 
 // Whole blocks [b0, b1) of a solve pass whose rows need no checks: one wait
 // per block, then its kRB rows, kU per step, with the refill after the last
-// rows are read.
+// rows are used.
 template <int F, int P, int PASS, bool DOWN>
 __device__ __forceinline__ void solve_blocks(const SumArgs& a, const PassPtrs<F>& p, const Lane& L, SumSmem& S,
                                              const Ops& o, int b0, int b1, SolveState<F>& st, RingPos& rp) {
@@ -761,16 +775,13 @@ __device__ __forceinline__ void solve_blocks(const SumArgs& a, const PassPtrs<F>
             RowF<F> f[kU];
 #pragma unroll
             for (int j = 0; j < kU; ++j) load_row<F, P, PASS>(blk, DOWN ? jj + j : kRB - 1 - jj - j, L, f[j]);
-            if (jj + kU == kRB) {
-                __syncwarp(L.wmask);
-                if (L.lane == 0 && b + NB < rp.nblk) ring_issue<F, P, PASS, DOWN>(a, L, S, b + NB, slot);
-            }
 #pragma unroll
             for (int j = 0; j < kU; ++j) {
                 const int r = row_of<DOWN>(L, b * kRB + jj + j);
                 if constexpr (PASS == kRefineUp) refine_row<F, P, false>(p, L, o, f[j], r, st);
                 else solve_row<F, P, PASS, DOWN, false>(p, L, o, f[j], r, st);
             }
+            if (jj + kU == kRB) ring_refill<F, P, PASS, DOWN>(a, L, S, b, slot, rp);
         }
         if (++slot == NB) {
             slot = 0;
@@ -792,9 +803,12 @@ __device__ void sum_pass(const SumArgs& a, const Lane& L, SumSmem& S, const Ops&
     const PassPtrs<F> p = pass_ptrs<F, DOWN>(a, L);
     RingCtl* ctl = ring_ctl(S);
     // The field, the workspace and the factors were last written by generic
-    // stores (the previous pass or factorisation) and the factor ring by
-    // cp.async; the bulk copies write and read through the async proxy.
-    __threadfence_block();
+    // stores of every lane (the previous pass or factorisation), and the
+    // factor ring by cp.async; lane 0's bulk copies read them through the
+    // async proxy, from L2.  Each lane's stores must have reached GPU scope
+    // (not only this CTA's view) before the copies are issued: the first
+    // rows a pass loads are the last ones the previous pass wrote.
+    __threadfence();
     fence_proxy_async();
     __syncwarp(L.wmask);
     RingPos rp;
