@@ -2,8 +2,8 @@
 //
 // The kernel templates of the batched march.  Each precision form is
 // instantiated in its own translation unit (march_sum_plain.cu,
-// march_sum_chosen.cu, march_sum_fast.cu) so that the three compile in
-// parallel; march_sum.cu dispatches on the form.
+// march_sum_chosen.cu, march_sum_fast.cu, march_sum_refined.cu) so that the
+// four compile in parallel; march_sum.cu dispatches on the form.
 //
 // The split-step Pade operator of one range step is a rational function of
 // the Galerkin operator X = M^{-1} D (M: mass matrix, D: Galerkin stiffness +
@@ -33,7 +33,8 @@
 // the tensor memory accelerator: one lane issues one bulk tensor copy per
 // field and block of kRB rows of the whole tile into a ring of blocks in
 // shared memory, completing on the block's mbarrier, which every lane waits
-// on before it reads the block.  Only 1/den and w are stored per term; the
+// on before it reads the block; a slot is refilled only after every lane has
+// used its rows.  Only 1/den and w are stored per term; the
 // elimination's coupling factor -(a1 + pd2 e) / den is rebuilt in FP64 from
 // 1/den and the row's Galerkin coupling e (d1 going down, d3 going up,
 // complex128), which is stored once per ray row and shared by the ray's
